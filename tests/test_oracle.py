@@ -1,0 +1,207 @@
+"""Pins of the CPU oracle (no GPU): exact dense evolution, independent generators, op algebra."""
+import numpy as np
+import pytest
+
+from oracle import dense as D
+from oracle import drivers as DR
+from oracle import models as M
+from oracle import mps_ref as R
+
+RNG = np.random.default_rng(1234)
+
+
+def crand(*shape):
+    return RNG.standard_normal(shape) + 1j * RNG.standard_normal(shape)
+
+
+# ---------------------------------------------------------------- op algebra
+
+def test_prod_AOR_matches_einsum():
+    A, O, Rr = crand(3, 2, 5), crand(4, 2, 6, 2), crand(5, 6, 7)
+    ref = np.einsum("asb,wtvs,bvc->awtc", A, O, Rr)
+    assert np.allclose(R.prod_AOR(A, O, Rr), ref, rtol=0, atol=1e-12)
+
+
+def test_prod_AOL_matches_einsum():
+    A, O, L = crand(3, 2, 5), crand(4, 2, 6, 2), crand(3, 4, 7)
+    ref = np.einsum("awx,asb,wtvs->xtbv", L.conj(), A, O)
+    assert np.allclose(R.prod_AOL(A, O, L), ref, rtol=0, atol=1e-12)
+
+
+def test_env_updates_match_einsum():
+    AOR, A0 = crand(3, 4, 2, 5), crand(6, 2, 5)
+    assert np.allclose(R.update_re(A0, AOR), np.einsum("awtc,xtc->awx", AOR, A0.conj()), atol=1e-12)
+    AOL, B0 = crand(6, 2, 5, 4), crand(6, 2, 3)
+    assert np.allclose(R.update_le(B0, AOL), np.einsum("xtbv,xty->bvy", AOL.conj(), B0), atol=1e-12)
+    A, FL, FR = crand(3, 2, 5), crand(4, 3), crand(5, 4)
+    AL = R.prod_LR(FL, A)
+    assert np.allclose(AL, np.einsum("xa,asb->xsb", FL, A), atol=1e-12)
+    C0 = crand(4, 2, 6)
+    assert np.allclose(R.update_lenv(C0, AL), np.einsum("xsy,xsb->yb", C0.conj(), AL), atol=1e-12)
+    assert np.allclose(R.update_lenv_nc(C0, AL), np.einsum("xsy,xsb->yb", C0, AL), atol=1e-12)
+    AR = R.prod_LR(A, FR)
+    D0 = crand(7, 2, 4)
+    assert np.allclose(R.update_renv(D0, AR), np.einsum("asb,xsb->ax", AR, D0.conj()), atol=1e-12)
+
+
+def test_qr_is_lapack_householder_convention():
+    X = crand(12, 5)
+    q, r = R.julia_qr(X)
+    assert np.allclose(q.conj().T @ q, np.eye(5), atol=1e-13)
+    assert np.allclose(q @ r, X, atol=1e-12)
+    # zlarfg makes the diagonal of R real with sign -sign(Re alpha) on the first column
+    assert np.allclose(np.imag(np.diag(r)), 0, atol=1e-14)
+    assert np.sign(r[0, 0].real) == -np.sign(X[0, 0].real)
+
+
+def test_rightorth_gives_right_orthonormal_site():
+    A = crand(4, 2, 3)
+    Q = R.rightorth_(A)
+    m = R.jr(Q, 4, 6)
+    assert np.allclose(m @ m.conj().T, np.eye(4), atol=1e-13)
+
+
+def test_dims_rule_and_product_state():
+    mps, dims = R.mpsgroundstate(10, 8, 2)
+    assert dims == R.dims_rule(10, 8, 2) == [1, 2, 4, 8, 8, 8, 8, 8, 4, 2, 1]
+    v = D.mps_to_dense(mps)
+    e = np.zeros(2 ** 10)
+    e[0] = 1
+    assert np.allclose(v, e, atol=1e-14)
+
+
+def test_mpo_algebra():
+    p = M.SpinChain(5, omega=0.3)
+    jr_, _ = M.jump_mpos(p)
+    c = R.conj_mpo(jr_)
+    prod = R.applyMPOtoMPO(jr_, c)
+    Jd, Cd, Pd = (D.mpo_to_dense(x) for x in (jr_, c, prod))
+    assert np.allclose(Cd, Jd.conj().T, atol=1e-13)
+    assert np.allclose(Pd, Cd @ Jd, atol=1e-13)
+    A, _ = R.mpsrandom(5, 4, 2, np.random.default_rng(3))
+    out = R.applyMPOtoMPS(A, jr_)
+    assert np.allclose(D.mps_to_dense(out), Jd @ D.mps_to_dense(A), atol=1e-12)
+
+
+# ---------------------------------------------------------------- generators
+
+def _op_at(o, i, n, d=2):
+    m = np.eye(1)
+    for j in range(n):
+        m = np.kron(m, o if j == i else np.eye(d))
+    return m
+
+
+def test_trajectory_generator_is_waveguide_heff():
+    n, phi, om = 6, 0.5 * np.pi, 0.5
+    p = M.SpinChain(n, k_wg=phi, omega=om)
+    G = D.mpo_to_dense(M.sm_hamiltonian(p, 0, 1, 0.0))
+    Heff = np.zeros((2 ** n, 2 ** n), complex)
+    for i in range(n):
+        Heff += -om * (_op_at(M.heg, i, n) + _op_at(M.hge, i, n))
+        for j in range(n):
+            Heff += -0.5j * np.exp(1j * phi * abs(i - j)) * _op_at(M.heg, i, n) @ _op_at(M.hge, j, n)
+    assert np.abs(G - (-1j) * Heff).max() < 1e-13
+
+
+def _dense_lindbladian(n, phi, om, gam, gam_eg, gam_phi):
+    """Superoperator on the per-site-interleaved vec(rho) used by the MPS ([gg,ge,eg,ee] per site)."""
+    D_ = 2 ** n
+    sp = [_op_at(M.heg, i, n) for i in range(n)]
+    sm = [_op_at(M.hge, i, n) for i in range(n)]
+    see = [_op_at(M.hee, i, n) for i in range(n)]
+    Heff = np.zeros((D_, D_), complex)
+    for i in range(n):
+        Heff += -om * (sp[i] + sm[i]) - 0.5j * (gam_eg + gam_phi) * see[i]
+        for j in range(n):
+            Heff += -0.5j * gam * np.exp(1j * phi * abs(i - j)) * sp[i] @ sm[j]
+    I = np.eye(D_)
+    Lsup = -1j * (np.kron(Heff, I) - np.kron(I, Heff.conj()))   # C-order vec: X rho Y -> X (x) Y^T
+    for i in range(n):
+        Lsup += gam_eg * np.kron(sm[i], sm[i].conj())
+        Lsup += gam_phi * np.kron(see[i], see[i].conj())
+        for j in range(n):
+            Lsup += gam * np.cos(phi * abs(i - j)) * np.kron(sm[j], sm[i].conj())
+    # reorder (a1..an, b1..bn) -> (a1 b1, ..., an bn)
+    perm = [x for k in range(n) for x in (k, n + k)]
+    T = Lsup.reshape([2] * (4 * n))
+    T = T.transpose(perm + [2 * n + q for q in perm])
+    return T.reshape(4 ** n, 4 ** n)
+
+
+def test_density_generator_is_lindbladian():
+    n, phi, om, gam_eg, gam_phi = 4, 0.5 * np.pi, 0.5, 0.1, 0.2
+    p = M.SpinChain(n, k_wg=phi, omega=om, gam_eg=gam_eg, gam_phi=gam_phi)
+    G = D.mpo_to_dense(M.construct_L_spin_model(p, 0, 1, 0.0))
+    Lref = _dense_lindbladian(n, phi, om, 1.0, gam_eg, gam_phi)
+    assert np.abs(G - Lref).max() < 1e-13
+    G8 = D.mpo_to_dense(M.construct_L_spin_model(p, 0, 1, 0.0, w=8))
+    assert np.abs(G8 - Lref).max() < 1e-13
+
+
+# ---------------------------------------------------------------- dense pins
+
+def test_rk4_trajectory_full_bond_matches_dense():
+    n, dt = 6, 0.01
+    p = M.SpinChain(n, omega=0.5)
+    A, dims = R.mpsgroundstate(n, 8, 2)
+    H = [M.sm_hamiltonian(p, 1, dt / 2, 0), M.sm_hamiltonian(p, 0, 1, dt / 2), M.sm_hamiltonian(p, 1, dt / 2, dt)]
+    Hd = [D.mpo_to_dense(h) for h in H]
+    psi = D.mps_to_dense(A)
+    A1, A2, A3, A0 = (R.copy_mps(A) for _ in range(4))
+    envop = R.build_env(dims, dims, [4] * (n + 1))
+    e1, e2, e3 = (R.build_env(dims, dims) for _ in range(3))
+    for _ in range(6):
+        R.RK4stp_apply_H_half_(dt, H, A0, A, A1, A2, A3, e1, e2, e3, envop)
+        psi = D.rk4_dense_step(*Hd, psi, dt)
+        assert np.abs(D.mps_to_dense(A0) - psi).max() < 1e-13
+        A = R.copy_mps(A0)
+    # RK4 algebra: psi + dt/6 (k1 + 2k2 + 2k3 + k4) for the time-independent generator
+    G = Hd[1]
+    v = D.mps_to_dense(R.mpsgroundstate(n, 8, 2)[0])
+    k1 = G @ v
+    k2 = G @ (v + dt / 2 * k1)
+    k3 = G @ (v + dt / 2 * k2)
+    k4 = G @ (v + dt * k3)
+    assert np.allclose(D.rk4_dense_step(*Hd, v, dt), v + dt / 6 * (k1 + 2 * k2 + 2 * k3 + k4), atol=1e-15)
+
+
+def test_rk4_density_full_bond_matches_dense_and_keeps_trace():
+    n, dt = 4, 0.005
+    p = M.SpinChain(n, gam_eg=0.1, omega=0.5, gam_phi=0.1)
+    rho, obs = DR.run_density(p, 16, dt, 6, w=8, measure_int=1)
+    L = [M.construct_L_spin_model(p, 1, dt / 2, 0, 8), M.construct_L_spin_model(p, 0, 1, dt / 2, 8),
+         M.construct_L_spin_model(p, 1, dt / 2, dt, 8)]
+    Ld = [D.mpo_to_dense(x) for x in L]
+    v = D.mps_to_dense(R.mpsgroundstate(n, 16, 4)[0])
+    for _ in range(6):
+        v = D.rk4_dense_step(*Ld, v, dt)
+    assert np.abs(D.mps_to_dense(rho) - v).max() < 1e-13
+    for tr, _, _ in obs:
+        assert abs(tr - 1) < 1e-13
+    # hermiticity of rho: rho_ab = conj(rho_ba)
+    Rm = v.reshape([2, 2] * n).transpose([2 * k for k in range(n)] + [2 * k + 1 for k in range(n)])
+    Rm = Rm.reshape(2 ** n, 2 ** n)
+    assert np.allclose(Rm, Rm.conj().T, atol=1e-14)
+
+
+def test_trajectory_probability_identity():
+    """p_coh + sum dt*p_jump = 1 + O(dt^2) (examples/spin_model_quantum_trajectory_rk4.jl:151)."""
+    n, dt = 6, 0.01
+    p = M.SpinChain(n, omega=0.5)
+    r1 = np.concatenate([np.zeros(40), np.ones(10)])   # coherent, then the jump branch every step
+    r2 = np.full(50, 0.3)
+    rec = DR.run_trajectory(p, 8, dt, 50, r1, r2, measure_int=5)
+    assert len(rec["jumps"]) == 10
+    assert max(j[4] for j in rec["jumps"]) > 1e-3
+    for (_, _, _, p_coh, p_sum) in rec["jumps"]:
+        assert abs(p_coh + p_sum - 1) < 2e-4
+
+
+@pytest.mark.parametrize("seed", [0])
+def test_trajectory_runs_and_normalises(seed):
+    p = M.SpinChain(8, omega=0.5)
+    r1, r2 = DR.uniforms(seed, 30)
+    rec = DR.run_trajectory(p, 8, 0.01, 30, r1, r2, measure_int=10)
+    assert abs(R.norm_lo(rec["A"]) - 1) < 1e-12
+    assert rec["e_pop"].shape == (4, 8)
