@@ -1,0 +1,179 @@
+/*
+ * mpsb.h -- C ABI of the mpsb200 engine: the RK4 MPS/MPO time step of
+ * jdnz/MatrixProductStates.jl on one B200 (sm_100a), complex128.
+ *
+ * Data conventions (the reference's own Julia layouts, so a Julia `ccall` can pass
+ * `pointer(A[j])` directly):
+ *   - complex numbers are interleaved (re, im) doubles  == Julia Complex{Float64}
+ *   - every tensor is column-major:
+ *       MPS site     A[chiL, d, chiR]                 (src/constructors.jl:19)
+ *       MPO site     O[wL, d_out, wR, d_in]           (src/constructors.jl:239-243)
+ *       3-index env  F[chi_A, w, chi_A0]              (src/constructors.jl:353)
+ *       2-index env  F[chi_1, chi_2]                  (src/constructors.jl:369)
+ *   - an MPS of `na` sites has bond dims dims[0..na] (dims[0] = dims[na] = 1);
+ *     an MPO has channel dims w[0..na] (w[0] = w[na] = 1).
+ *
+ * Conventions of the interface:
+ *   - every entry point returns int status: MPSB_OK (0) or a negative MPSB_ERR_*;
+ *     mpsb_last_error() gives a message for the calling thread.
+ *   - the library owns device memory behind opaque handles; the caller owns host buffers.
+ *   - a context owns one CUDA stream; calls are asynchronous on it unless they return a
+ *     host value (norms, scalar products), which synchronise.  A context is used by one
+ *     host thread at a time.
+ *   - there is no CPU fallback: without a usable sm_100 device, mpsb_ctx_create fails.
+ */
+#ifndef MPSB_H
+#define MPSB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  MPSB_OK = 0,
+  MPSB_ERR_INVALID_ARG = -1,      /* null handle / pointer, bad enum */
+  MPSB_ERR_DIMENSION = -2,        /* shapes do not match (Julia: DimensionMismatch) */
+  MPSB_ERR_CUDA = -3,             /* a CUDA runtime call failed */
+  MPSB_ERR_OUT_OF_MEMORY = -4,    /* device allocation failed */
+  MPSB_ERR_UNSUPPORTED = -5,      /* size outside what the kernels implement */
+  MPSB_ERR_NONFINITE = -6,        /* a norm or probability came out NaN/Inf */
+  MPSB_ERR_NO_DEVICE = -7         /* no CUDA device with compute capability 10.x */
+};
+
+typedef struct mpsb_ctx mpsb_ctx;
+typedef struct mpsb_mps mpsb_mps;
+typedef struct mpsb_mpo mpsb_mpo;
+typedef struct mpsb_env mpsb_env;
+
+/* ---------------------------------------------------------------- context */
+const char* mpsb_last_error(void);
+int mpsb_version(void);
+int mpsb_ctx_create(int device, mpsb_ctx** out);
+int mpsb_ctx_destroy(mpsb_ctx* ctx);
+int mpsb_sync(mpsb_ctx* ctx);
+/* Use an external CUDA stream (cudaStream_t passed as void*); NULL restores the own stream. */
+int mpsb_ctx_set_stream(mpsb_ctx* ctx, void* stream);
+/* Capture each RK4 step into a CUDA graph and replay it (default on). */
+int mpsb_ctx_set_graphs(mpsb_ctx* ctx, int enable);
+/* Kernel launches issued by this context since creation (for accounting). */
+int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out);
+
+/* ---------------------------------------------------------------- MPS (Vector{Array{T,3}}) */
+int mpsb_mps_create(mpsb_ctx* ctx, int na, int d, const int64_t* dims /* na+1 */, mpsb_mps** out);
+int mpsb_mps_destroy(mpsb_mps* A);
+int mpsb_mps_info(const mpsb_mps* A, int* na, int* d, int64_t* dims /* na+1, may be NULL */);
+/* site is 1-based like the reference; host buffer holds dims[site-1]*d*dims[site] complex */
+int mpsb_mps_set_site(mpsb_mps* A, int site, const double* host);
+int mpsb_mps_get_site(const mpsb_mps* A, int site, double* host);
+/* device pointer of a site (for zero-copy interop); site 1-based */
+int mpsb_mps_site_ptr(const mpsb_mps* A, int site, void** dptr);
+/* dst .= copy.(src)  (examples/spin_model_quantum_trajectory_rk4.jl:130) */
+int mpsb_mps_copy(mpsb_mps* dst, const mpsb_mps* src);
+
+/* ---------------------------------------------------------------- MPO (Vector{Array{T,4}}) */
+int mpsb_mpo_create(mpsb_ctx* ctx, int na, int d, const int64_t* w /* na+1 */, mpsb_mpo** out);
+int mpsb_mpo_destroy(mpsb_mpo* O);
+int mpsb_mpo_set_site(mpsb_mpo* O, int site, const double* host);
+int mpsb_mpo_get_site(const mpsb_mpo* O, int site, double* host);
+
+/* ---------------------------------------------------------------- environments
+ * build_env(TN, TA, dims1, dims2[, mpo_dims])  src/constructors.jl:347-375
+ * w == NULL gives 2-index envs; ends are ones(1,1[,1]), interior zeros. */
+int mpsb_env_create(mpsb_ctx* ctx, int na, const int64_t* dims1, const int64_t* dims2,
+                    const int64_t* w /* na+1 or NULL */, mpsb_env** out);
+int mpsb_env_destroy(mpsb_env* E);
+/* entry is 1-based (1..na+1) like env[jj] in the reference */
+int mpsb_env_get(const mpsb_env* E, int entry, double* host);
+int mpsb_env_set(mpsb_env* E, int entry, const double* host);
+
+/* ---------------------------------------------------------------- the RK4 hot path
+ * RK4stp_apply_H_half!(dt, H, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop)
+ *   src/timeevolution.jl:188-196 (11-arg); psi0 == psi gives the 10-arg in-place form
+ *   src/timeevolution.jl:178-186.  H1, H2, H3 are H[1], H[2], H[3]. */
+int mpsb_rk4stp_apply_H_half(mpsb_ctx* ctx, double dt,
+                             const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
+                             mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2,
+                             mpsb_mps* psi3, mpsb_env* env1, mpsb_env* env2, mpsb_env* env3,
+                             mpsb_env* envop);
+
+/* compress_var_apply_H_left!(A0, envop, Ain, A, H)   src/compression.jl:321-347 */
+int mpsb_compress_var_apply_H_left(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop,
+                                   const mpsb_mps* Ain, const mpsb_mps* A, const mpsb_mpo* H);
+
+/* compress_sum_var_apply_H_right!(A0, env, envop, Ain, coef, A, H)  src/compression.jl:1007-1063
+ * compress_sum_var_apply_H_left!(A0, env, envop, Ain, coef, A, H)   src/compression.jl:889-944
+ * numv = length(coef) = length(A); env has numv-1 entries; coef is numv interleaved complex;
+ * A[numv-1] is the MPS the operator H acts on. A0 may equal A[0] (read before written). */
+int mpsb_compress_sum_var_apply_H_right(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* const* env,
+                                        mpsb_env* envop, const mpsb_mps* Ain, const double* coef,
+                                        int numv, mpsb_mps* const* A, const mpsb_mpo* H);
+int mpsb_compress_sum_var_apply_H_left(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* const* env,
+                                       mpsb_env* envop, const mpsb_mps* Ain, const double* coef,
+                                       int numv, mpsb_mps* const* A, const mpsb_mpo* H);
+
+/* compress_var_apply_H!(A0, envop, Ain, A, H, maxsweeps)  src/compression.jl:217-258
+ * (jump-operator application in the trajectory driver) */
+int mpsb_compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain,
+                              const mpsb_mps* A, const mpsb_mpo* H, int maxsweeps);
+
+/* ---------------------------------------------------------------- gauge / norms
+ * normalize_lo!(mps) src/orthonormalisation.jl:97-103 -> *no = sum(abs2, mps[end])
+ * norm_lo(mps)       src/orthonormalisation.jl:117-121
+ * leftorthonormalizationQR!(mps) src/orthonormalisation.jl:29-36 (returns the norm^2) */
+int mpsb_normalize_lo(mpsb_ctx* ctx, mpsb_mps* A, double* no);
+int mpsb_norm_lo(mpsb_ctx* ctx, const mpsb_mps* A, double* no);
+int mpsb_leftorthonormalizationQR(mpsb_ctx* ctx, mpsb_mps* A, double* no);
+/* leftorthogonalizeQR!(mps) src/orthonormalisation.jl:43-56: the same QR sweep with R carried
+ * right, returning the norm^2 without rescaling (mpsproductstate / expandmps use this sweep) */
+int mpsb_leftorthogonalizeQR(mpsb_ctx* ctx, mpsb_mps* A, double* no);
+/* apply_site_operator!(A[site], op)  src/MatrixProductStates.jl:135-143; op is d x d column-major */
+int mpsb_apply_site_operator(mpsb_ctx* ctx, mpsb_mps* A, int site, const double* op);
+
+/* ---------------------------------------------------------------- observables
+ * scal_prod(A, B)          src/MatrixProductStates.jl:345-358   <A|B>
+ * scal_op_prod(A, O, B)    src/MatrixProductStates.jl:327-340   <A|O|B>
+ * scal_prod_no_conj(A, B)  src/MatrixProductStates.jl:366-379   sum A.B (no conjugation)
+ * measure_local(A, op)     examples/spin_model_quantum_trajectory_rk4.jl:220-231
+ *                          (measure_excitations!: right-to-left local_exp sweep, mps_base.jl:341-349),
+ *                          out[na] = real(local <op_n>) for a left-orthonormal MPS. */
+int mpsb_scal_prod(mpsb_ctx* ctx, const mpsb_mps* A, const mpsb_mps* B, double* out /* 2 */);
+int mpsb_scal_op_prod(mpsb_ctx* ctx, const mpsb_mps* A, const mpsb_mpo* O, const mpsb_mps* B,
+                      double* out /* 2 */);
+int mpsb_scal_prod_no_conj(mpsb_ctx* ctx, const mpsb_mps* A, const mpsb_mps* B, double* out /* 2 */);
+int mpsb_measure_local(mpsb_ctx* ctx, const mpsb_mps* A, const double* op /* d x d */, double* out);
+
+/* applyMPOtoMPS(mps, mpo)  src/MatrixProductStates.jl:115-133 (exact, bond dims multiply);
+ * out must have dims[k]*w[k] bonds. */
+int mpsb_apply_mpo_to_mps(mpsb_ctx* ctx, const mpsb_mps* A, const mpsb_mpo* O, mpsb_mps* out);
+
+/* ---------------------------------------------------------------- op level (device pointers)
+ * Raw device buffers in the Julia layouts above, for op-by-op parity checks and for callers
+ * that manage their own memory.  Outputs are written, never accumulated. */
+/* prod_AOR(A, O, R) -> AOR[chiL, wL, d, chiR0]      src/mps_base.jl:7-19 */
+int mpsb_op_prod_AOR(mpsb_ctx* ctx, const void* A, const void* O, const void* R, void* AOR,
+                     int chiL, int d, int chiR, int wL, int wR, int chiR0);
+/* prod_AOL(A, O, L) -> AOL[chiL0, d, chiR, wR]      src/mps_base.jl:26-39 */
+int mpsb_op_prod_AOL(mpsb_ctx* ctx, const void* A, const void* O, const void* L, void* AOL,
+                     int chiL, int d, int chiR, int wL, int wR, int chiL0);
+/* prod_LR!(A0, L, AOR): A0[chiL0, d, chiR0] = L' * AOR   src/mps_base.jl:53-61 */
+int mpsb_op_prod_LR_3_4(mpsb_ctx* ctx, const void* L, const void* AOR, void* A0,
+                        int chiL, int wL, int chiL0, int d, int chiR0);
+/* prod_LR!(A0, AOL, R): A0 = AOL * R                     src/mps_base.jl:73-81 */
+int mpsb_op_prod_LR_4_3(mpsb_ctx* ctx, const void* AOL, const void* R, void* A0,
+                        int chiL0, int d, int chiR, int wR, int chiR0);
+/* update_re!(env, A0, AOR): env[chiL, wL, chiL0]         src/mps_base.jl:151-160 */
+int mpsb_op_update_re(mpsb_ctx* ctx, const void* A0, const void* AOR, void* env,
+                      int chiL, int wL, int d, int chiR0, int chiL0);
+/* update_le!(env, A0, AOL): env[chiR, wR, chiR0]         src/mps_base.jl:232-241 */
+int mpsb_op_update_le(mpsb_ctx* ctx, const void* A0, const void* AOL, void* env,
+                      int chiL0, int d, int chiR, int wR, int chiR0);
+/* Q of the LAPACK geqrf+orgqr QR of the column-major m x n matrix X (m >= n):
+ * qrq!(X)  src/orthonormalisation.jl:180-184. Q may alias X. R (n x n) optional (NULL). */
+int mpsb_op_qr(mpsb_ctx* ctx, const void* X, void* Q, void* R, int m, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPSB_H */

@@ -1,0 +1,433 @@
+// Sweep orchestration: the reference's contraction helpers (src/mps_base.jl), gauge moves
+// (src/orthonormalisation.jl) and compression sweeps (src/compression.jl) expressed as
+// launches of the strided GEMM, MPO-apply and cluster-QR kernels on the context stream.
+#include <algorithm>
+#include <cstring>
+
+#include "engine.cuh"
+
+namespace mpsb {
+
+int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out) {
+  DevBuf& b = ctx->ws.named[s];
+  void* before = b.p;
+  MPSB_TRY(devbuf_ensure(&ctx->ws, b, bytes));
+  if (b.p != before) ctx->ws_generation++;
+  *out = static_cast<cd*>(b.p);
+  return MPSB_OK;
+}
+
+static inline int run_gemm(mpsb_ctx* ctx, const Gemm& g) {
+  void* before = ctx->ws.splitk.p;
+  int st = gemm_launch(g, &ctx->ws, ctx->stream);
+  if (ctx->ws.splitk.p != before) ctx->ws_generation++;
+  return st;
+}
+
+static inline int run_mpo(mpsb_ctx* ctx, const MpoApply& a, int64_t k1, int64_t k2, int64_t m1, int64_t m2) {
+  count_launch(&ctx->ws);
+  return mpo_apply_launch_strided(a, k1, k2, m1, m2, ctx->stream);
+}
+
+static const cd ONE = {1.0, 0.0};
+static const cd ZERO = {0.0, 0.0};
+
+// prod_AOR (src/mps_base.jl:7-19): T = A*R (GEMM), AOR = O . T (small-K apply, permutes folded)
+int op_prod_AOR(mpsb_ctx* ctx, const cd* A, const cd* O, const cd* R, cd* AOR, int chiL, int d, int chiR, int wL,
+                int wR, int chiR0) {
+  cd* T;
+  MPSB_TRY(ensure_slot(ctx, SLOT_T, (size_t)chiL * d * wR * chiR0 * sizeof(cd), &T));
+  Gemm g;
+  g.M = chiL * d; g.N = wR * chiR0; g.K = chiR;
+  g.A = A; g.a_m = 1; g.a_k = (int64_t)chiL * d;
+  g.B = R; g.b_k = 1; g.b_n = chiR;
+  g.C = T; g.c_m = 1; g.c_n = (int64_t)chiL * d;
+  MPSB_TRY(run_gemm(ctx, g));
+  MpoApply a;
+  a.X = chiL; a.Y = chiR0; a.K1 = d; a.K2 = wR; a.M1 = wL; a.M2 = d;
+  a.in = T; a.in_x = 1; a.in_k1 = chiL; a.in_k2 = (int64_t)chiL * d; a.in_y = (int64_t)chiL * d * wR;
+  a.op = O;
+  a.out = AOR; a.out_x = 1; a.out_m1 = chiL; a.out_m2 = (int64_t)chiL * wL; a.out_y = (int64_t)chiL * wL * d;
+  return run_mpo(ctx, a, (int64_t)wL * d * wR, (int64_t)wL * d, 1, wL);
+}
+
+// prod_AOL (src/mps_base.jl:26-39): G1 = L' * A (GEMM), AOL = G1 . O
+int op_prod_AOL(mpsb_ctx* ctx, const cd* A, const cd* O, const cd* L, cd* AOL, int chiL, int d, int chiR, int wL,
+                int wR, int chiL0) {
+  cd* G1;
+  MPSB_TRY(ensure_slot(ctx, SLOT_G1, (size_t)wL * chiL0 * d * chiR * sizeof(cd), &G1));
+  Gemm g;
+  g.M = wL * chiL0; g.N = d * chiR; g.K = chiL;
+  g.A = L; g.a_m = chiL; g.a_k = 1; g.conjA = true;
+  g.B = A; g.b_k = 1; g.b_n = chiL;
+  g.C = G1; g.c_m = 1; g.c_n = (int64_t)wL * chiL0;
+  MPSB_TRY(run_gemm(ctx, g));
+  MpoApply a;
+  a.X = chiL0; a.Y = chiR; a.K1 = wL; a.K2 = d; a.M1 = d; a.M2 = wR;
+  a.in = G1; a.in_x = wL; a.in_k1 = 1; a.in_k2 = (int64_t)wL * chiL0; a.in_y = (int64_t)wL * chiL0 * d;
+  a.op = O;
+  a.out = AOL; a.out_x = 1; a.out_m1 = chiL0; a.out_m2 = (int64_t)chiL0 * d * chiR; a.out_y = (int64_t)chiL0 * d;
+  return run_mpo(ctx, a, 1, (int64_t)wL * d * wR, wL, (int64_t)wL * d);
+}
+
+// prod_LR!(A0, L, AOR) (src/mps_base.jl:53-61): A0 = L' * AOR
+int op_prod_LR_3_4(mpsb_ctx* ctx, const cd* L, const cd* AOR, cd* A0, int chiL, int wL, int chiL0, int d, int chiR0,
+                   cd alpha, cd beta) {
+  Gemm g;
+  g.M = chiL0; g.N = d * chiR0; g.K = chiL * wL;
+  g.A = L; g.a_m = (int64_t)chiL * wL; g.a_k = 1; g.conjA = true;
+  g.B = AOR; g.b_k = 1; g.b_n = (int64_t)chiL * wL;
+  g.C = A0; g.c_m = 1; g.c_n = chiL0;
+  g.alpha = alpha; g.beta = beta;
+  return run_gemm(ctx, g);
+}
+
+// prod_LR!(A0, AOL, R) (src/mps_base.jl:73-81): A0 = AOL * R
+int op_prod_LR_4_3(mpsb_ctx* ctx, const cd* AOL, const cd* R, cd* A0, int chiL0, int d, int chiR, int wR, int chiR0,
+                   cd alpha, cd beta) {
+  Gemm g;
+  g.M = chiL0 * d; g.N = chiR0; g.K = chiR * wR;
+  g.A = AOL; g.a_m = 1; g.a_k = (int64_t)chiL0 * d;
+  g.B = R; g.b_k = 1; g.b_n = (int64_t)chiR * wR;
+  g.C = A0; g.c_m = 1; g.c_n = (int64_t)chiL0 * d;
+  g.alpha = alpha; g.beta = beta;
+  return run_gemm(ctx, g);
+}
+
+// update_re!(env, A0, AOR) (src/mps_base.jl:151-160): env = AOR * A0'
+int op_update_re(mpsb_ctx* ctx, const cd* A0, const cd* AOR, cd* env, int chiL, int wL, int d, int chiR0, int chiL0) {
+  Gemm g;
+  g.M = chiL * wL; g.N = chiL0; g.K = d * chiR0;
+  g.A = AOR; g.a_m = 1; g.a_k = (int64_t)chiL * wL;
+  g.B = A0; g.b_k = chiL0; g.b_n = 1; g.conjB = true;
+  g.C = env; g.c_m = 1; g.c_n = (int64_t)chiL * wL;
+  return run_gemm(ctx, g);
+}
+
+// update_le!(env, A0, AOL) (src/mps_base.jl:232-241): env = AOL' * A0
+int op_update_le(mpsb_ctx* ctx, const cd* A0, const cd* AOL, cd* env, int chiL0, int d, int chiR, int wR, int chiR0) {
+  Gemm g;
+  g.M = chiR * wR; g.N = chiR0; g.K = chiL0 * d;
+  g.A = AOL; g.a_m = (int64_t)chiL0 * d; g.a_k = 1; g.conjA = true;
+  g.B = A0; g.b_k = 1; g.b_n = (int64_t)chiL0 * d;
+  g.C = env; g.c_m = 1; g.c_n = (int64_t)chiR * wR;
+  return run_gemm(ctx, g);
+}
+
+// prod_LR(L2, A3) (src/mps_base.jl:85-90, 100-108): out(x, rest) = L(x, chiL) * A(chiL, rest);
+// transL gives prod_LR_co (L.')
+int op_L2_A3(mpsb_ctx* ctx, const cd* L, const cd* A, cd* out, int x, int chiL, int rest, cd alpha, cd beta,
+             bool transL) {
+  Gemm g;
+  g.M = x; g.N = rest; g.K = chiL;
+  g.A = L;
+  if (transL) { g.a_m = chiL; g.a_k = 1; } else { g.a_m = 1; g.a_k = x; }
+  g.B = A; g.b_k = 1; g.b_n = chiL;
+  g.C = out; g.c_m = 1; g.c_n = x;
+  g.alpha = alpha; g.beta = beta;
+  return run_gemm(ctx, g);
+}
+
+// prod_LR(A3, R2) (src/mps_base.jl:122-137): out(lead, y) = A(lead, chiR) * R(chiR, y)
+int op_A3_R2(mpsb_ctx* ctx, const cd* A, const cd* R, cd* out, int lead, int chiR, int y, cd alpha, cd beta) {
+  Gemm g;
+  g.M = lead; g.N = y; g.K = chiR;
+  g.A = A; g.a_m = 1; g.a_k = lead;
+  g.B = R; g.b_k = 1; g.b_n = chiR;
+  g.C = out; g.c_m = 1; g.c_n = lead;
+  g.alpha = alpha; g.beta = beta;
+  return run_gemm(ctx, g);
+}
+
+// update_renv!(env, A0, AR) (src/mps_base.jl:193-199): env(chiA, chiL0) = AR(chiA, drest) * A0(chiL0, drest)'
+int op_update_renv(mpsb_ctx* ctx, const cd* A0, const cd* AR, cd* env, int chiA, int chiL0, int drest) {
+  Gemm g;
+  g.M = chiA; g.N = chiL0; g.K = drest;
+  g.A = AR; g.a_m = 1; g.a_k = chiA;
+  g.B = A0; g.b_k = chiL0; g.b_n = 1; g.conjB = true;
+  g.C = env; g.c_m = 1; g.c_n = chiA;
+  return run_gemm(ctx, g);
+}
+
+// update_lenv!(env, A0, AL) (src/mps_base.jl:275-281) and update_lenv_nc (:319-325):
+// env(chiR0, y) = A0(lead, chiR0)' * AL(lead, y)   (.' when !conj)
+int op_update_lenv(mpsb_ctx* ctx, const cd* A0, const cd* AL, cd* env, int lead, int chiR0, int y, bool conj) {
+  Gemm g;
+  g.M = chiR0; g.N = y; g.K = lead;
+  g.A = A0; g.a_m = lead; g.a_k = 1; g.conjA = conj;
+  g.B = AL; g.b_k = 1; g.b_n = lead;
+  g.C = env; g.c_m = 1; g.c_n = chiR0;
+  return run_gemm(ctx, g);
+}
+
+// leftorth! / leftorth (src/orthonormalisation.jl:150-171): Q of reshape(A, Dl*d, Dr), in place
+int op_orth_left(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr, cd* R) {
+  QrProblem p;
+  p.m = Dl * d; p.n = Dr;
+  p.X = A; p.x_r = 1; p.x_c = (int64_t)Dl * d;
+  p.Q = A; p.q_r = 1; p.q_c = (int64_t)Dl * d;
+  if (R) { p.R = R; p.r_r = 1; p.r_c = Dr; }
+  count_launch(&ctx->ws);
+  return qr_launch(p, ctx->stream);
+}
+
+// rightorth! (src/orthonormalisation.jl:227-234): QR of the non-conjugate transpose
+// reshape(A, Dl, d*Dr).' and A = reshape(Q.', Dl, d, Dr), in place
+int op_orth_right(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr) {
+  QrProblem p;
+  p.m = d * Dr; p.n = Dl;
+  p.X = A; p.x_r = Dl; p.x_c = 1;
+  p.Q = A; p.q_r = Dl; p.q_c = 1;
+  count_launch(&ctx->ws);
+  return qr_launch(p, ctx->stream);
+}
+
+// ------------------------------------------------------------------------------------
+static int same_dims(const mpsb_mps* a, const mpsb_mps* b) {
+  return a && b && a->na == b->na && a->d == b->d && a->dims == b->dims;
+}
+
+static int set_boundary(mpsb_ctx* ctx, cd* p, cd v) {
+  count_launch(&ctx->ws);
+  return set_value(p, v, ctx->stream);
+}
+
+struct SweepScratch {
+  cd* AOR; cd* AOL; cd* P[8];
+};
+
+static int sweep_scratch(mpsb_ctx* ctx, const mpsb_mps* A0, const mpsb_mpo* H, int nplain, SweepScratch& s) {
+  int64_t maxAOR = 1, maxAOL = 1, maxSite = 1;
+  const int d = A0->d;
+  for (int k = 0; k < A0->na; ++k) {
+    int64_t Dl = A0->dims[k], Dr = A0->dims[k + 1];
+    maxAOR = std::max<int64_t>(maxAOR, Dl * H->w[k] * d * Dr);
+    maxAOL = std::max<int64_t>(maxAOL, Dl * d * Dr * H->w[k + 1]);
+    maxSite = std::max<int64_t>(maxSite, Dl * d * Dr);
+  }
+  MPSB_TRY(ensure_slot(ctx, SLOT_AOR, maxAOR * sizeof(cd), &s.AOR));
+  MPSB_TRY(ensure_slot(ctx, SLOT_AOL, maxAOL * sizeof(cd), &s.AOL));
+  if (nplain > 8) return MPSB_ERR_UNSUPPORTED;
+  cd* base = nullptr;
+  if (nplain > 0) MPSB_TRY(ensure_slot(ctx, SLOT_P0, (size_t)nplain * maxSite * sizeof(cd), &base));
+  for (int i = 0; i < nplain; ++i) s.P[i] = base + (int64_t)i * maxSite;
+  return MPSB_OK;
+}
+
+// compress_sum_var_apply_H_left! (src/compression.jl:889-944) when !right,
+// compress_sum_var_apply_H_right! (src/compression.jl:1007-1063) when right.
+// numv == 1 with coef {1} is compress_var_apply_H_left! (src/compression.jl:321-347).
+int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* const* env, mpsb_env* envop,
+                             const mpsb_mps* Ain, const cd* coef, int numv, const mpsb_mps* const* A,
+                             const mpsb_mpo* H) {
+  if (!ctx || !A0 || !envop || !Ain || !coef || !A || !H || numv < 1) return MPSB_ERR_INVALID_ARG;
+  const int np = numv - 1;
+  if (!same_dims(A0, Ain)) return MPSB_ERR_DIMENSION;
+  for (int l = 0; l < numv; ++l)
+    if (!same_dims(A0, A[l])) return MPSB_ERR_DIMENSION;
+  for (int l = 0; l < np; ++l)
+    if (!env || !env[l] || env[l]->three || env[l]->na != A0->na) return MPSB_ERR_DIMENSION;
+  if (!envop->three || envop->na != A0->na || H->na != A0->na || H->d != A0->d) return MPSB_ERR_DIMENSION;
+  const int na = A0->na, d = A0->d;
+  for (int k = 0; k <= na; ++k) {
+    if (envop->d1[k] != A0->dims[k] || envop->d2[k] != A0->dims[k] || envop->w[k] != H->w[k]) return MPSB_ERR_DIMENSION;
+    for (int l = 0; l < np; ++l)
+      if (env[l]->d1[k] != A0->dims[k] || env[l]->d2[k] != A0->dims[k]) return MPSB_ERR_DIMENSION;
+  }
+  SweepScratch s;
+  MPSB_TRY(sweep_scratch(ctx, A0, H, np, s));
+  const mpsb_mps* AH = A[np];
+  auto D = [&](int k) { return (int)A0->dims[k]; };
+  auto W = [&](int k) { return (int)H->w[k]; };
+
+  if (!right) {
+    // ---- left environments from Ain (bra) and the terms (kets)
+    for (int l = 0; l < np; ++l) {
+      MPSB_TRY(set_boundary(ctx, env[l]->entry(0), ONE));
+      for (int k = 0; k < na - 1; ++k) {
+        MPSB_TRY(op_L2_A3(ctx, env[l]->entry(k), A[l]->site(k), s.P[l], D(k), D(k), d * D(k + 1), ONE, ZERO, false));
+        MPSB_TRY(op_update_lenv(ctx, Ain->site(k), s.P[l], env[l]->entry(k + 1), D(k) * d, D(k + 1), D(k + 1), true));
+      }
+      MPSB_TRY(set_boundary(ctx, env[l]->entry(na), coef[l]));
+    }
+    MPSB_TRY(set_boundary(ctx, envop->entry(0), ONE));
+    for (int k = 0; k < na - 1; ++k) {
+      MPSB_TRY(op_prod_AOL(ctx, AH->site(k), H->site(k), envop->entry(k), s.AOL, D(k), d, D(k + 1), W(k), W(k + 1), D(k)));
+      MPSB_TRY(op_update_le(ctx, Ain->site(k), s.AOL, envop->entry(k + 1), D(k), d, D(k + 1), W(k + 1), D(k + 1)));
+    }
+    MPSB_TRY(set_boundary(ctx, envop->entry(na), coef[np]));
+    // ---- right-to-left half sweep
+    for (int k = na - 1; k >= 0; --k) {
+      cd* out = A0->site(k);
+      for (int l = 0; l < np; ++l) {
+        MPSB_TRY(op_A3_R2(ctx, A[l]->site(k), env[l]->entry(k + 1), s.P[l], D(k) * d, D(k + 1), D(k + 1), ONE, ZERO));
+        MPSB_TRY(op_L2_A3(ctx, env[l]->entry(k), s.P[l], out, D(k), D(k), d * D(k + 1), ONE, l ? ONE : ZERO, false));
+      }
+      MPSB_TRY(op_prod_AOR(ctx, AH->site(k), H->site(k), envop->entry(k + 1), s.AOR, D(k), d, D(k + 1), W(k), W(k + 1), D(k + 1)));
+      MPSB_TRY(op_prod_LR_3_4(ctx, envop->entry(k), s.AOR, out, D(k), W(k), D(k), d, D(k + 1), ONE, np ? ONE : ZERO));
+      if (k == 0) break;
+      MPSB_TRY(op_orth_right(ctx, out, D(k), d, D(k + 1)));
+      for (int l = 0; l < np; ++l)
+        MPSB_TRY(op_update_renv(ctx, out, s.P[l], env[l]->entry(k), D(k), D(k), d * D(k + 1)));
+      MPSB_TRY(op_update_re(ctx, out, s.AOR, envop->entry(k), D(k), W(k), d, D(k + 1), D(k)));
+    }
+  } else {
+    // ---- right environments
+    for (int l = 0; l < np; ++l) {
+      MPSB_TRY(set_boundary(ctx, env[l]->entry(na), ONE));
+      for (int k = na - 1; k >= 1; --k) {
+        MPSB_TRY(op_A3_R2(ctx, A[l]->site(k), env[l]->entry(k + 1), s.P[l], D(k) * d, D(k + 1), D(k + 1), ONE, ZERO));
+        MPSB_TRY(op_update_renv(ctx, Ain->site(k), s.P[l], env[l]->entry(k), D(k), D(k), d * D(k + 1)));
+      }
+      MPSB_TRY(set_boundary(ctx, env[l]->entry(0), coef[l]));
+    }
+    MPSB_TRY(set_boundary(ctx, envop->entry(na), ONE));
+    for (int k = na - 1; k >= 1; --k) {
+      MPSB_TRY(op_prod_AOR(ctx, AH->site(k), H->site(k), envop->entry(k + 1), s.AOR, D(k), d, D(k + 1), W(k), W(k + 1), D(k + 1)));
+      MPSB_TRY(op_update_re(ctx, Ain->site(k), s.AOR, envop->entry(k), D(k), W(k), d, D(k + 1), D(k)));
+    }
+    MPSB_TRY(set_boundary(ctx, envop->entry(0), coef[np]));
+    // ---- left-to-right half sweep
+    for (int k = 0; k < na; ++k) {
+      cd* out = A0->site(k);
+      for (int l = 0; l < np; ++l) {
+        MPSB_TRY(op_L2_A3(ctx, env[l]->entry(k), A[l]->site(k), s.P[l], D(k), D(k), d * D(k + 1), ONE, ZERO, false));
+        MPSB_TRY(op_A3_R2(ctx, s.P[l], env[l]->entry(k + 1), out, D(k) * d, D(k + 1), D(k + 1), ONE, l ? ONE : ZERO));
+      }
+      MPSB_TRY(op_prod_AOL(ctx, AH->site(k), H->site(k), envop->entry(k), s.AOL, D(k), d, D(k + 1), W(k), W(k + 1), D(k)));
+      MPSB_TRY(op_prod_LR_4_3(ctx, s.AOL, envop->entry(k + 1), out, D(k), d, D(k + 1), W(k + 1), D(k + 1), ONE, np ? ONE : ZERO));
+      if (k == na - 1) break;
+      MPSB_TRY(op_orth_left(ctx, out, D(k), d, D(k + 1), nullptr));
+      for (int l = 0; l < np; ++l)
+        MPSB_TRY(op_update_lenv(ctx, out, s.P[l], env[l]->entry(k + 1), D(k) * d, D(k + 1), D(k + 1), true));
+      MPSB_TRY(op_update_le(ctx, out, s.AOL, envop->entry(k + 1), D(k), d, D(k + 1), W(k + 1), D(k + 1)));
+    }
+  }
+  return MPSB_OK;
+}
+
+int compress_var_apply_H_left(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain, const mpsb_mps* A,
+                              const mpsb_mpo* H) {
+  const mpsb_mps* terms[1] = {A};
+  cd c1[1] = {ONE};
+  return compress_sum_var_apply_H(ctx, false, A0, nullptr, envop, Ain, c1, 1, terms, H);
+}
+
+// compress_var_apply_H! (src/compression.jl:217-258): maxsweeps R->L / L->R sweep pairs
+int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain, const mpsb_mps* A,
+                         const mpsb_mpo* H, int maxsweeps) {
+  if (!ctx || !A0 || !envop || !Ain || !A || !H || maxsweeps < 0) return MPSB_ERR_INVALID_ARG;
+  if (!same_dims(A0, Ain) || !same_dims(A0, A) || !envop->three || H->na != A0->na) return MPSB_ERR_DIMENSION;
+  const int na = A0->na, d = A0->d;
+  for (int k = 0; k <= na; ++k)
+    if (envop->d1[k] != A0->dims[k] || envop->d2[k] != A0->dims[k] || envop->w[k] != H->w[k]) return MPSB_ERR_DIMENSION;
+  SweepScratch s;
+  MPSB_TRY(sweep_scratch(ctx, A0, H, 0, s));
+  auto D = [&](int k) { return (int)A0->dims[k]; };
+  auto W = [&](int k) { return (int)H->w[k]; };
+  MPSB_TRY(set_boundary(ctx, envop->entry(0), ONE));
+  for (int k = 0; k < na - 1; ++k) {
+    MPSB_TRY(op_prod_AOL(ctx, A->site(k), H->site(k), envop->entry(k), s.AOL, D(k), d, D(k + 1), W(k), W(k + 1), D(k)));
+    MPSB_TRY(op_update_le(ctx, Ain->site(k), s.AOL, envop->entry(k + 1), D(k), d, D(k + 1), W(k + 1), D(k + 1)));
+  }
+  MPSB_TRY(set_boundary(ctx, envop->entry(na), ONE));
+  for (int sw = 0; sw < maxsweeps; ++sw) {
+    for (int k = na - 1; k >= 1; --k) {
+      MPSB_TRY(op_prod_AOR(ctx, A->site(k), H->site(k), envop->entry(k + 1), s.AOR, D(k), d, D(k + 1), W(k), W(k + 1), D(k + 1)));
+      MPSB_TRY(op_prod_LR_3_4(ctx, envop->entry(k), s.AOR, A0->site(k), D(k), W(k), D(k), d, D(k + 1), ONE, ZERO));
+      MPSB_TRY(op_orth_right(ctx, A0->site(k), D(k), d, D(k + 1)));
+      MPSB_TRY(op_update_re(ctx, A0->site(k), s.AOR, envop->entry(k), D(k), W(k), d, D(k + 1), D(k)));
+    }
+    for (int k = 0; k < na; ++k) {
+      MPSB_TRY(op_prod_AOL(ctx, A->site(k), H->site(k), envop->entry(k), s.AOL, D(k), d, D(k + 1), W(k), W(k + 1), D(k)));
+      MPSB_TRY(op_prod_LR_4_3(ctx, s.AOL, envop->entry(k + 1), A0->site(k), D(k), d, D(k + 1), W(k + 1), D(k + 1), ONE, ZERO));
+      if (k == na - 1) break;
+      MPSB_TRY(op_orth_left(ctx, A0->site(k), D(k), d, D(k + 1), nullptr));
+      MPSB_TRY(op_update_le(ctx, A0->site(k), s.AOL, envop->entry(k + 1), D(k), d, D(k + 1), W(k + 1), D(k + 1)));
+    }
+  }
+  return MPSB_OK;
+}
+
+// RK4stp_apply_H_half! (src/timeevolution.jl:178-196)
+static int rk4_body(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
+                    mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3, mpsb_env* env1,
+                    mpsb_env* env2, mpsb_env* env3, mpsb_env* envop) {
+  MPSB_TRY(compress_var_apply_H_left(ctx, psi1, envop, psi, psi, H1));
+  {
+    mpsb_env* e[1] = {env1};
+    const mpsb_mps* t[2] = {psi, psi1};
+    cd c[2] = {ONE, cmk(dt / 2, 0.0)};
+    MPSB_TRY(compress_sum_var_apply_H(ctx, true, psi2, e, envop, psi1, c, 2, t, H2));
+  }
+  {
+    mpsb_env* e[1] = {env1};
+    const mpsb_mps* t[2] = {psi, psi2};
+    cd c[2] = {ONE, cmk(dt, 0.0)};
+    MPSB_TRY(compress_sum_var_apply_H(ctx, false, psi3, e, envop, psi2, c, 2, t, H2));
+  }
+  {
+    mpsb_env* e[3] = {env1, env2, env3};
+    const mpsb_mps* t[4] = {psi, psi1, psi2, psi3};
+    cd c[4] = {cmk(-1.0 / 3, 0.0), cmk(1.0 / 3, 0.0), cmk(2.0 / 3, 0.0), cmk(1.0 / 3, 0.0)};
+    MPSB_TRY(compress_sum_var_apply_H(ctx, true, psi0, e, envop, psi3, c, 4, t, H3));
+  }
+  return MPSB_OK;
+}
+
+int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3, mpsb_mps* psi0,
+             mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3, mpsb_env* env1, mpsb_env* env2,
+             mpsb_env* env3, mpsb_env* envop) {
+  if (!ctx || !H1 || !H2 || !H3 || !psi0 || !psi || !psi1 || !psi2 || !psi3 || !env1 || !env2 || !env3 || !envop)
+    return MPSB_ERR_INVALID_ARG;
+  if (!ctx->graphs)
+    return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
+  int64_t dtbits;
+  std::memcpy(&dtbits, &dt, sizeof(dt));
+  std::vector<int64_t> key = {1, dtbits, H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial,
+                              psi1->serial, psi2->serial, psi3->serial, env1->serial, env2->serial,
+                              env3->serial, envop->serial};
+  auto& ent = ctx->graphs_cache[key];
+  if (ent.exec && ent.generation == ctx->ws_generation) {
+    ctx->ws.launches += 0;  // replay: launches already counted at capture
+    MPSB_CUDA_TRY(cudaGraphLaunch(ent.exec, ctx->stream));
+    return MPSB_OK;
+  }
+  if (ent.exec) {
+    cudaGraphExecDestroy(ent.exec);
+    ent.exec = nullptr;
+    ent.seen = 0;
+  }
+  if (ent.seen == 0) {  // eager first call sizes every scratch buffer
+    ent.seen = 1;
+    return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
+  }
+  const int64_t gen0 = ctx->ws_generation;
+  ctx->ws.capturing = true;
+  MPSB_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int st = rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
+  cudaGraph_t g = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->ws.capturing = false;
+  if (st != MPSB_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (ce != cudaSuccess) {
+    set_last_error(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+    return MPSB_ERR_CUDA;
+  }
+  cudaGraphExec_t exec = nullptr;
+  ce = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    set_last_error(ce, "cudaGraphInstantiate", __FILE__, __LINE__);
+    return MPSB_ERR_CUDA;
+  }
+  ent.exec = exec;
+  ent.generation = gen0;
+  MPSB_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
+  return MPSB_OK;
+}
+
+}  // namespace mpsb

@@ -1,0 +1,111 @@
+// Handles and host-side sweep orchestration of the mpsb200 engine.
+#pragma once
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "common.cuh"
+#include "misc.cuh"
+#include "workspace.cuh"
+
+struct mpsb_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  mpsb::Workspace ws;
+  bool graphs = true;
+  int64_t ws_generation = 0;   // bumped whenever a scratch buffer is reallocated
+  double* d_scalars = nullptr; // small device scratch for norms (64 doubles)
+  double* h_scalars = nullptr; // pinned host mirror
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    int64_t generation = -1;
+    int seen = 0;
+  };
+  std::map<std::vector<int64_t>, GraphEntry> graphs_cache;
+};
+
+struct mpsb_mps {
+  mpsb_ctx* ctx = nullptr;
+  int64_t serial = 0;
+  int na = 0, d = 0;
+  std::vector<int64_t> dims;   // na+1
+  std::vector<int64_t> off;    // element offset of each site
+  mpsb::cd* slab = nullptr;
+  int64_t total = 0;
+  mpsb::cd* site(int s) const { return slab + off[s]; }
+  int64_t site_elems(int s) const { return dims[s] * d * dims[s + 1]; }
+};
+
+struct mpsb_mpo {
+  mpsb_ctx* ctx = nullptr;
+  int64_t serial = 0;
+  int na = 0, d = 0;
+  std::vector<int64_t> w;      // na+1
+  std::vector<int64_t> off;
+  mpsb::cd* slab = nullptr;
+  int64_t total = 0;
+  mpsb::cd* site(int s) const { return slab + off[s]; }
+  int64_t site_elems(int s) const { return w[s] * d * w[s + 1] * d; }
+};
+
+struct mpsb_env {
+  mpsb_ctx* ctx = nullptr;
+  int64_t serial = 0;
+  int na = 0;
+  bool three = false;
+  std::vector<int64_t> d1, d2, w;  // na+1 each (w all 1 for 2-index)
+  std::vector<int64_t> off;
+  mpsb::cd* slab = nullptr;
+  int64_t total = 0;
+  mpsb::cd* entry(int e) const { return slab + off[e]; }
+  int64_t entry_elems(int e) const { return d1[e] * w[e] * d2[e]; }
+};
+
+namespace mpsb {
+
+// named scratch slots in Workspace::named
+enum Slot {
+  SLOT_T = 0, SLOT_AOR, SLOT_G1, SLOT_AOL, SLOT_P0, SLOT_P1, SLOT_P2, SLOT_ENV0, SLOT_ENV1,
+  SLOT_MISC, SLOT_COUNT
+};
+
+int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out);
+
+// ---- single contractions (device pointers, dims explicit); alpha/beta accumulate into out
+int op_prod_AOR(mpsb_ctx* ctx, const cd* A, const cd* O, const cd* R, cd* AOR, int chiL, int d, int chiR,
+                int wL, int wR, int chiR0);
+int op_prod_AOL(mpsb_ctx* ctx, const cd* A, const cd* O, const cd* L, cd* AOL, int chiL, int d, int chiR,
+                int wL, int wR, int chiL0);
+int op_prod_LR_3_4(mpsb_ctx* ctx, const cd* L, const cd* AOR, cd* A0, int chiL, int wL, int chiL0, int d,
+                   int chiR0, cd alpha, cd beta);
+int op_prod_LR_4_3(mpsb_ctx* ctx, const cd* AOL, const cd* R, cd* A0, int chiL0, int d, int chiR, int wR,
+                   int chiR0, cd alpha, cd beta);
+int op_update_re(mpsb_ctx* ctx, const cd* A0, const cd* AOR, cd* env, int chiL, int wL, int d, int chiR0,
+                 int chiL0);
+int op_update_le(mpsb_ctx* ctx, const cd* A0, const cd* AOL, cd* env, int chiL0, int d, int chiR, int wR,
+                 int chiR0);
+// 2-index env products
+int op_L2_A3(mpsb_ctx* ctx, const cd* L, const cd* A, cd* out, int x, int chiL, int rest, cd alpha, cd beta,
+             bool transL);
+int op_A3_R2(mpsb_ctx* ctx, const cd* A, const cd* R, cd* out, int lead, int chiR, int y, cd alpha, cd beta);
+int op_update_renv(mpsb_ctx* ctx, const cd* A0, const cd* AR, cd* env, int chiA, int chiL0, int drest);
+int op_update_lenv(mpsb_ctx* ctx, const cd* A0, const cd* AL, cd* env, int lead, int chiR0, int y, bool conj);
+// QR of a site: left (reshape(A, Dl*d, Dr)) or right (transpose of reshape(A, Dl, d*Dr))
+int op_orth_left(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr, cd* R /* Dr x Dr or null */);
+int op_orth_right(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr);
+
+// ---- sweeps (the reference's compress_* family)
+int compress_var_apply_H_left(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain,
+                              const mpsb_mps* A, const mpsb_mpo* H);
+int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* const* env, mpsb_env* envop,
+                             const mpsb_mps* Ain, const cd* coef, int numv, const mpsb_mps* const* A,
+                             const mpsb_mpo* H);
+int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain, const mpsb_mps* A,
+                         const mpsb_mpo* H, int maxsweeps);
+int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
+             mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3, mpsb_env* env1,
+             mpsb_env* env2, mpsb_env* env3, mpsb_env* envop);
+
+}  // namespace mpsb

@@ -1,0 +1,50 @@
+// Device scratch owned by one context.  Buffers only grow; growth is refused while a CUDA
+// graph is being captured (the first, eager call of a step sizes everything).
+#pragma once
+#include "common.cuh"
+
+namespace mpsb {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct Workspace {
+  DevBuf splitk;          // split-K partial tiles
+  DevBuf named[16];       // per-sweep temporaries (see engine.cu)
+  bool capturing = false;
+  int64_t launches = 0;   // kernel launches issued (eager) or recorded (capture)
+};
+
+inline void count_launch(Workspace* ws) {
+  if (ws) ws->launches++;
+}
+
+inline int devbuf_ensure(Workspace* ws, DevBuf& b, size_t bytes) {
+  if (bytes <= b.cap) return MPSB_OK;
+  if (ws && ws->capturing) {
+    set_last_message("workspace growth (%zu bytes) requested during graph capture", bytes);
+    return MPSB_ERR_UNSUPPORTED;
+  }
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  size_t want = bytes + bytes / 4 + 4096;
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    set_last_error(e, "cudaMalloc(workspace)", __FILE__, __LINE__);
+    return MPSB_ERR_OUT_OF_MEMORY;
+  }
+  b.cap = want;
+  return MPSB_OK;
+}
+
+inline int ws_splitk(Workspace* ws, size_t bytes, cd** out) {
+  if (!ws) return MPSB_ERR_INVALID_ARG;
+  MPSB_TRY(devbuf_ensure(ws, ws->splitk, bytes));
+  *out = static_cast<cd*>(ws->splitk.p);
+  return MPSB_OK;
+}
+
+}  // namespace mpsb
