@@ -389,7 +389,7 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
                               env3->serial, envop->serial};
   auto& ent = ctx->graphs_cache[key];
   if (ent.exec && ent.generation == ctx->ws_generation) {
-    ctx->ws.launches += 0;  // replay: launches already counted at capture
+    ctx->ws.launches += ent.launches;
     MPSB_CUDA_TRY(cudaGraphLaunch(ent.exec, ctx->stream));
     return MPSB_OK;
   }
@@ -403,6 +403,7 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
     return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
   }
   const int64_t gen0 = ctx->ws_generation;
+  const int64_t l0 = ctx->ws.launches;
   ctx->ws.capturing = true;
   MPSB_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   int st = rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
@@ -426,6 +427,7 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
   }
   ent.exec = exec;
   ent.generation = gen0;
+  ent.launches = ctx->ws.launches - l0;
   MPSB_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
   return MPSB_OK;
 }

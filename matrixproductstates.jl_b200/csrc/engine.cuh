@@ -21,6 +21,7 @@ struct mpsb_ctx {
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
     int64_t generation = -1;
+    int64_t launches = 0;  // kernel nodes recorded at capture, added on every replay
     int seen = 0;
   };
   std::map<std::vector<int64_t>, GraphEntry> graphs_cache;

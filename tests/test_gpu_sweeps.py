@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from gpu_util import relerr
+from gpu_util import fidelity, perturbed_oracle_qr, relerr
 from oracle import dense as D
 from oracle import drivers as ODR
 from oracle import models as OM
@@ -118,8 +118,10 @@ def test_rk4_trajectory_step_matches_oracle_and_dense(gpu_ctx):
         K.RK4stp_apply_H_half_(dt, gH, g0, gA, g1, g2, g3, *ge, gop)
         psi = D.rk4_dense_step(*Hd, psi, dt)
         got = D.mps_to_dense(g0.sites())
+        # the state itself (gauge invariant); raw sites may differ by the gauge of zero-weight
+        # columns at exactly rank-deficient bonds (signed zeros decide a Householder sign there)
         assert np.abs(got - psi).max() < 1e-12
-        _sites_close(g0, A0, 1e-10)
+        assert np.abs(D.mps_to_dense(A0) - psi).max() < 1e-12
         A = R.copy_mps(A0)
         gA.copy_from(g0)
 
@@ -137,7 +139,7 @@ def test_rk4_density_inplace_matches_oracle(gpu_ctx):
         assert abs(tr - tr_r) < 1e-10
         assert np.abs(see - see_r).max() < 1e-10
         assert np.abs(spm - spm_r).max() < 1e-10
-    _sites_close(b.rho, rho_ref, 1e-8)
+    assert 1 - fidelity(b.rho.sites(), rho_ref) < 1e-12
 
 
 def test_observables_match_oracle(gpu_ctx):
@@ -178,11 +180,18 @@ def test_trajectory_with_jumps_matches_oracle(gpu_ctx):
     r1, r2 = ODR.uniforms(3, nsteps)
     r1 = np.where(np.arange(nsteps) % 7 == 6, 1.0, 0.0)       # force a jump every 7th step
     ref = ODR.run_trajectory(OM.SpinChain(na, omega=0.5), chi, dt, nsteps, r1, r2, measure_int=10)
+    with perturbed_oracle_qr(1e-15):
+        pert = ODR.run_trajectory(OM.SpinChain(na, omega=0.5), chi, dt, nsteps, r1, r2, measure_int=10)
     got = GDR.run_trajectory(GM.WaveguideChain(na, omega=0.5), chi, dt, nsteps, r1, r2, measure_int=10, ctx=gpu_ctx)
     assert [j[:3] for j in got["jumps"]] == [j[:3] for j in ref["jumps"]]
     assert len(ref["jumps"]) >= 5
-    assert np.abs(got["p_coh"] - ref["p_coh"]).max() < 1e-10
-    assert np.abs(got["e_pop"] - ref["e_pop"]).max() < 1e-9
+    # chi=16 < 2^5 truncates: the oracle itself moves by env under rounding-level perturbations of
+    # its QR inputs; the GPU must stay within a small multiple of that envelope
+    env_p = np.abs(pert["p_coh"] - ref["p_coh"]).max()
+    env_e = np.abs(pert["e_pop"] - ref["e_pop"]).max()
+    assert np.abs(got["p_coh"] - ref["p_coh"]).max() < 1e-12 + 100 * env_p
+    assert np.abs(got["e_pop"] - ref["e_pop"]).max() < 1e-12 + 100 * env_e
+    assert np.abs(got["p_coh"][:20] - ref["p_coh"][:20]).max() < 1e-12
 
 
 def test_graph_replay_is_bitwise_eager(gpu_ctx):
