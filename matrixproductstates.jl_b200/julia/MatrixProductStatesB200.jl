@@ -1,0 +1,146 @@
+# Julia-side shim: the reference's RK4 hot-path API on top of libmpsb200 (ccall).
+#
+# UNVERIFIED: Julia is not installed in the build image, so this file has never been run.
+# It targets Julia >= 1.6 (the reference itself needs Julia 0.6.4, whose `ccall` syntax is
+# the same).  Host tensors keep the reference layouts (Array{ComplexF64,3} sites,
+# Array{ComplexF64,4} MPO sites), so `pointer(A[j])` is passed straight to the C ABI.
+module MatrixProductStatesB200
+
+const LIB = joinpath(@__DIR__, "..", "mpsb200", "libmpsb200.so")
+
+struct MpsbError <: Exception
+    status::Cint
+    func::Symbol
+    msg::String
+end
+
+function check(st, f)
+    st == 0 && return nothing
+    msg = unsafe_string(ccall((:mpsb_last_error, LIB), Cstring, ()))
+    st == -2 && throw(DimensionMismatch("$f: $msg"))
+    throw(MpsbError(st, f, msg))
+end
+
+mutable struct Ctx
+    h::Ptr{Cvoid}
+end
+function Ctx(device::Integer = 0)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:mpsb_ctx_create, LIB), Cint, (Cint, Ptr{Ptr{Cvoid}}), device, r), :mpsb_ctx_create)
+    c = Ctx(r[])
+    finalizer(x -> ccall((:mpsb_ctx_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), c)
+    return c
+end
+
+# Device MPS / MPO / env handles ("TA = GPU" of the reference's TN/TA type parameters)
+mutable struct DMPS
+    h::Ptr{Cvoid}
+    dims::Vector{Int64}
+    d::Int
+end
+mutable struct DMPO
+    h::Ptr{Cvoid}
+    w::Vector{Int64}
+    d::Int
+end
+mutable struct DEnv
+    h::Ptr{Cvoid}
+end
+
+function DMPS(ctx::Ctx, A::Vector{<:Array{ComplexF64,3}})
+    dims = Int64[1; [size(a, 3) for a in A]]
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:mpsb_mps_create, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Int64}, Ptr{Ptr{Cvoid}}),
+                ctx.h, length(A), size(A[1], 2), dims, r), :mpsb_mps_create)
+    m = DMPS(r[], dims, size(A[1], 2))
+    for (j, a) in enumerate(A)
+        check(ccall((:mpsb_mps_set_site, LIB), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), m.h, j, a),
+              :mpsb_mps_set_site)
+    end
+    finalizer(x -> ccall((:mpsb_mps_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), m)
+    return m
+end
+
+function collect_sites(m::DMPS)
+    na = length(m.dims) - 1
+    out = Vector{Array{ComplexF64,3}}(undef, na)
+    for j in 1:na
+        a = Array{ComplexF64,3}(undef, m.dims[j], m.d, m.dims[j+1])
+        check(ccall((:mpsb_mps_get_site, LIB), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), m.h, j, a),
+              :mpsb_mps_get_site)
+        out[j] = a
+    end
+    return out
+end
+
+function DMPO(ctx::Ctx, O::Vector{<:Array{ComplexF64,4}})
+    w = Int64[1; [size(o, 3) for o in O]]
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:mpsb_mpo_create, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Int64}, Ptr{Ptr{Cvoid}}),
+                ctx.h, length(O), size(O[1], 2), w, r), :mpsb_mpo_create)
+    m = DMPO(r[], w, size(O[1], 2))
+    for (j, o) in enumerate(O)
+        check(ccall((:mpsb_mpo_set_site, LIB), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), m.h, j, o),
+              :mpsb_mpo_set_site)
+    end
+    finalizer(x -> ccall((:mpsb_mpo_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), m)
+    return m
+end
+
+# update_h!/update_L_spin_model! refresh one MPO site in place (same device buffer)
+set_site!(m::DMPO, j::Integer, o::Array{ComplexF64,4}) =
+    check(ccall((:mpsb_mpo_set_site, LIB), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), m.h, j, o), :mpsb_mpo_set_site)
+
+# build_env(TN, TA, dims1, dims2[, mpo_dims])   src/constructors.jl:347-375
+function build_env(ctx::Ctx, dims1::Vector{<:Integer}, dims2::Vector{<:Integer}, mpo_dims = nothing)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    wptr = mpo_dims === nothing ? Ptr{Int64}(C_NULL) : pointer(Int64.(mpo_dims))
+    w = mpo_dims === nothing ? Int64[] : Int64.(mpo_dims)
+    GC.@preserve w begin
+        check(ccall((:mpsb_env_create, LIB), Cint,
+                    (Ptr{Cvoid}, Cint, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Ptr{Cvoid}}),
+                    ctx.h, length(dims1) - 1, Int64.(dims1), Int64.(dims2),
+                    mpo_dims === nothing ? C_NULL : pointer(w), r), :mpsb_env_create)
+    end
+    e = DEnv(r[])
+    finalizer(x -> ccall((:mpsb_env_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), e)
+    return e
+end
+
+# RK4stp_apply_H_half!(dt, H, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop)
+#   src/timeevolution.jl:188-196; the 10-argument in-place form passes psi twice.
+function RK4stp_apply_H_half!(ctx::Ctx, dt::Real, H::Vector{DMPO}, psi0::DMPS, psi::DMPS, psi1::DMPS,
+                              psi2::DMPS, psi3::DMPS, env1::DEnv, env2::DEnv, env3::DEnv, envop::DEnv)
+    check(ccall((:mpsb_rk4stp_apply_H_half, LIB), Cint,
+                (Ptr{Cvoid}, Cdouble, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid},
+                 Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}),
+                ctx.h, dt, H[1].h, H[2].h, H[3].h, psi0.h, psi.h, psi1.h, psi2.h, psi3.h,
+                env1.h, env2.h, env3.h, envop.h), :mpsb_rk4stp_apply_H_half)
+end
+RK4stp_apply_H_half!(ctx::Ctx, dt::Real, H::Vector{DMPO}, psi::DMPS, psi1::DMPS, psi2::DMPS, psi3::DMPS,
+                     env1::DEnv, env2::DEnv, env3::DEnv, envop::DEnv) =
+    RK4stp_apply_H_half!(ctx, dt, H, psi, psi, psi1, psi2, psi3, env1, env2, env3, envop)
+
+# compress_var_apply_H!(A0, envop, Ain, A, H, maxsweeps)   src/compression.jl:217-258
+compress_var_apply_H!(ctx::Ctx, A0::DMPS, envop::DEnv, Ain::DMPS, A::DMPS, H::DMPO, maxsweeps::Integer) =
+    check(ccall((:mpsb_compress_var_apply_H, LIB), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Cint),
+                ctx.h, A0.h, envop.h, Ain.h, A.h, H.h, maxsweeps), :mpsb_compress_var_apply_H)
+
+# normalize_lo!(mps)   src/orthonormalisation.jl:97-103
+function normalize_lo!(ctx::Ctx, A::DMPS)
+    no = Ref{Cdouble}(0)
+    check(ccall((:mpsb_normalize_lo, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Cdouble}), ctx.h, A.h, no),
+          :mpsb_normalize_lo)
+    return no[]
+end
+
+# scal_prod_no_conj(mps1, mps2)   src/MatrixProductStates.jl:366-379
+function scal_prod_no_conj(ctx::Ctx, A::DMPS, B::DMPS)
+    out = zeros(Cdouble, 2)
+    check(ccall((:mpsb_scal_prod_no_conj, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cdouble}),
+                ctx.h, A.h, B.h, out), :mpsb_scal_prod_no_conj)
+    return complex(out[1], out[2])
+end
+
+end # module
