@@ -169,6 +169,19 @@ int mpsb_op_update_re(mpsb_ctx* ctx, const void* A0, const void* AOR, void* env,
 /* update_le!(env, A0, AOL): env[chiR, wR, chiR0]         src/mps_base.jl:232-241 */
 int mpsb_op_update_le(mpsb_ctx* ctx, const void* A0, const void* AOL, void* env,
                       int chiL0, int d, int chiR, int wR, int chiR0);
+/* prod_AOR for callers that cannot allocate device memory. No counterpart in the reference:
+ * it exists for hosts whose device memory belongs to their own pool allocator (a Julia
+ * CUDA.jl or PyTorch caching allocator) or that must not call cudaMalloc/cudaFree in their
+ * time loop, since those synchronise the device.  Same result as mpsb_op_prod_AOR, but it
+ * takes a CUDA stream (cudaStream_t as void*) instead of a context and calls no cudaMalloc,
+ * cudaFree or allocating routine: its one intermediate, A*R, lives in a fixed 16 MiB array
+ * compiled into the library (held on every GPU that loads the library until exit), so
+ * chiL*d*wR*chiR0 must be <= 1048576, else it returns MPSB_ERR_UNSUPPORTED.  The first call
+ * on a device looks up that array's device address (make the device current first, and make
+ * that first call before any stream capture).  All calls share the array: calls that overlap
+ * on the GPU (other streams, other host threads) race; serialise them on one stream. */
+int mpsb_op_prod_AOR_noalloc(void* stream, const void* A, const void* O, const void* R, void* AOR,
+                             int chiL, int d, int chiR, int wL, int wR, int chiR0);
 /* Q of the LAPACK geqrf+orgqr QR of the column-major m x n matrix X (m >= n):
  * qrq!(X)  src/orthonormalisation.jl:180-184. Q may alias X. R (n x n) optional (NULL). */
 int mpsb_op_qr(mpsb_ctx* ctx, const void* X, void* Q, void* R, int m, int n);

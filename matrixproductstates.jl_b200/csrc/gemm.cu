@@ -224,7 +224,8 @@ int gemm_launch(const Gemm& g, Workspace* ws, cudaStream_t s) {
   const int64_t ctas = (int64_t)tiles * g.batch;
   int splits = 1;
   const int target = 2 * 148;  // two resident 64x64 tiles per SM
-  if (ctas < target && KT >= 8) {
+  // without a workspace (ws == nullptr) K is never split, so no scratch is needed
+  if (ws && ctas < target && KT >= 8) {
     splits = (int)std::min<int64_t>((target + ctas - 1) / ctas, KT / 4);
     splits = std::max(1, std::min(splits, 32));
   }

@@ -73,6 +73,7 @@ SIGNATURES = {
     "mpsb_op_update_re": ([_vp] * 4 + [_i] * 5, _i),
     "mpsb_op_update_le": ([_vp] * 4 + [_i] * 5, _i),
     "mpsb_op_qr": ([_vp] * 4 + [_i] * 2, _i),
+    "mpsb_op_prod_AOR_noalloc": ([_vp] * 5 + [_i] * 6, _i),
 }
 
 _lib = None
