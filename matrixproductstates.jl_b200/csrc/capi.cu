@@ -33,7 +33,16 @@ static int bind(mpsb_ctx* ctx) {
 }
 
 static int sync(mpsb_ctx* ctx) {
+  int* hw = reinterpret_cast<int*>(ctx->h_scalars + 63);
+  MPSB_CUDA_TRY(cudaMemcpyAsync(hw, ctx->err(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   MPSB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (*hw != 0) {
+    *hw = 0;
+    cudaMemsetAsync(ctx->err(), 0, sizeof(int), ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    set_last_message("a device-side exchange wait timed out (QR cluster kernel); results of this stream are invalid");
+    return MPSB_ERR_CUDA;
+  }
   return MPSB_OK;
 }
 
@@ -121,6 +130,8 @@ int mpsb_ctx_create(int device, mpsb_ctx** out) {
     set_last_message("allocation of context scalars failed");
     return MPSB_ERR_OUT_OF_MEMORY;
   }
+  cudaMemset(c->d_scalars, 0, 64 * sizeof(double));
+  c->h_scalars[63] = 0.0;
   *out = c;
   return MPSB_OK;
 }
@@ -588,6 +599,7 @@ int mpsb_op_qr(mpsb_ctx* ctx, const void* X, void* Q, void* R, int m, int n) {
   p.X = DP(X); p.x_r = 1; p.x_c = m;
   p.Q = DW(Q); p.q_r = 1; p.q_c = m;
   if (R) { p.R = DW(R); p.r_r = 1; p.r_c = n; }
+  p.err = ctx->err();
   count_launch(&ctx->ws);
   return qr_launch(p, ctx->stream);
 }

@@ -97,6 +97,7 @@ struct QrProblem {
   const cd* X = nullptr; int64_t x_r = 0, x_c = 0, x_b = 0;   // input element strides (row, col, batch)
   cd* Q = nullptr;       int64_t q_r = 0, q_c = 0, q_b = 0;   // output (may alias X with equal strides)
   cd* R = nullptr;       int64_t r_r = 0, r_c = 0, r_b = 0;   // optional n x n upper-triangular factor
+  int* err = nullptr;    // device word; a bounded wait that runs out sets bit 0 (may be null)
 };
 int qr_launch(const QrProblem& p, cudaStream_t s);
 bool qr_supported(int m, int n);

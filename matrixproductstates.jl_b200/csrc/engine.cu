@@ -167,6 +167,7 @@ int op_orth_left(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr, cd* R) {
   p.X = A; p.x_r = 1; p.x_c = (int64_t)Dl * d;
   p.Q = A; p.q_r = 1; p.q_c = (int64_t)Dl * d;
   if (R) { p.R = R; p.r_r = 1; p.r_c = Dr; }
+  p.err = ctx->err();
   count_launch(&ctx->ws);
   return qr_launch(p, ctx->stream);
 }
@@ -178,6 +179,7 @@ int op_orth_right(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr) {
   p.m = d * Dr; p.n = Dl;
   p.X = A; p.x_r = Dl; p.x_c = 1;
   p.Q = A; p.q_r = Dl; p.q_c = 1;
+  p.err = ctx->err();
   count_launch(&ctx->ws);
   return qr_launch(p, ctx->stream);
 }

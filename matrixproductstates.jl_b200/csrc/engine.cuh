@@ -18,6 +18,8 @@ struct mpsb_ctx {
   int64_t ws_generation = 0;   // bumped whenever a scratch buffer is reallocated
   double* d_scalars = nullptr; // small device scratch for norms (64 doubles)
   double* h_scalars = nullptr; // pinned host mirror
+  // device error word (inside d_scalars[63]): kernels whose bounded waits run out set bit 0
+  int* err() const { return reinterpret_cast<int*>(d_scalars + 63); }
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
     int64_t generation = -1;

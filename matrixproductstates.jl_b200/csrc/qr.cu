@@ -6,22 +6,29 @@
 //   else beta = -copysign(|(alpha, x)|, Re alpha), tau = (beta - alpha)/beta,
 //        v = [1; x/(alpha - beta)], R[j,j] = beta (real)
 // H(j)^H = I - conj(tau) v v^H is applied to the trailing columns (zgeqr2), and
-// Q = H(1)...H(n) [I; 0] (zungqr).  Because only the span of Q carries physics in the
-// sweeps, the one convention that must match LAPACK exactly is the sign / phase rule
-// above, which also fixes the "junk" columns of zero-padded (rank-deficient) sites.
+// Q = H(1)...H(n) [I; 0] (zungqr).  Only the span of Q carries physics in the sweeps; the
+// sign / phase rule above is what must match LAPACK, and it also fixes the "junk" columns of
+// zero-padded (rank-deficient) sites.
 //
-// B200 mapping: one thread-block cluster per matrix; the m rows are split over the C
-// CTAs of the cluster (ROWS rows each, the whole matrix lives in distributed shared
-// memory).  Blocked right-looking algorithm with panels of nb columns:
-//   * panel column j: every CTA reduces its rows (norm, dot products with the remaining
-//     panel columns, and V^H x for the compact-WY factor T), one cluster barrier, every
-//     CTA gathers the C partial sets over DSMEM in a fixed order (so all CTAs compute
-//     bit-identical reflectors) and updates its rows;
-//   * trailing columns: W = V^H A partials -> barrier -> reduce-scatter + T^H ->
-//     barrier -> all-gather -> A -= V W (two barriers per panel);
-//   * Q formation runs the panels backwards with Q_trail -= V (T (V^H Q_trail)) and the
-//     panel block built directly as E - V (T V1^H) (two barriers per panel).
-// All reductions are in a fixed order: results are reproducible run to run.
+// B200 mapping: one thread-block cluster per matrix, rows split over its C CTAs (32*RPL
+// rows each; the whole matrix lives in distributed shared memory).  Blocked right-looking
+// algorithm with panels of NB columns.  Every exchange between CTAs is a *push*: the
+// producer writes its values straight into each consumer's shared memory with st.async,
+// whose completion is counted in bytes on the consumer's mbarrier; the consumer waits on
+// its own mbarrier (bounded) and then reads only local shared memory.  No cluster-wide
+// barrier sits inside the loops.
+//   * column j: each warp reduces its panel columns over the CTA's rows with warp shuffles
+//     (lane = row) and pushes the sums to all C CTAs; the owner of row j pushes that row;
+//     after the wait every warp recomputes the reflector, w = v^H A and the new column of
+//     the compact-WY factor T redundantly in registers, and updates its columns;
+//   * trailing columns: partials of V^H A pushed to the owner of each column slice,
+//     reduced there in a fixed order with T^H applied, the slice pushed to every CTA,
+//     then A -= V W locally;
+//   * Q formation runs the panels backwards: Q_trail -= V (T (V^H Q_trail)) with the same
+//     two exchanges, the panel block built as E - V (T V1^H) from the pushed top block V1.
+// Reductions run in a fixed order, so every CTA computes bit-identical reflectors and
+// results are reproducible run to run.  Each wait gives up after a bounded number of polls,
+// records the timeout in the error word and lets the kernel run to completion.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -34,233 +41,380 @@ namespace cg = cooperative_groups;
 namespace mpsb {
 namespace {
 
-constexpr int NT = 256;
+constexpr int NT = 256, NW = 8;
+constexpr int CMAX = 16;
 constexpr size_t SMEM_LIMIT = 227 * 1024;
+constexpr int WAIT_LIMIT = 1 << 22;
+enum { MB_COL0 = 0, MB_COL1, MB_RS, MB_AG, MB_V10, MB_V11, MB_COUNT };
 
 struct QrParams {
   QrProblem p;
-  int C, rows, nb, npanels, ldS;
-  // shared-memory offsets (in complex elements)
-  int o_S, o_step, o_bc, o_wpart, o_w2s, o_T, o_v1pub, o_v1loc, o_mloc, o_red;
-  int step_elems, w2s_cols;
+  int C, npanels, ldS, ksmax;
+  // shared-memory offsets (complex elements) and the byte offset of the mbarriers
+  int o_S, o_rcol, o_rrs, o_w2s, o_rag, o_T, o_rv1, o_mloc, o_bc, o_tst, o_mbar;
 };
 
-// ---- per-CTA shared memory map ------------------------------------------------------
-// S      [(rows+1) * n]   local rows of the matrix, column-major, ld = rows+1
-// step   2 x [2*nb]       pq[nb] (partial dot products), rowj[nb] (published row j)
-// bc     [4 + 4*nb]       tau, beta, scale, pad, w[nb], t[nb], sumpq[nb], rowjl[nb]
-// wpart  [nb * n]         trailing partials V^H A (this CTA's rows); reused as the gathered W2
-// w2s    [nb * w2s_cols]  this CTA's reduced slice of W2
-// T      [npanels*nb*nb]  compact-WY triangular factors of all panels
-// v1pub / v1loc / mloc [nb*nb]  panel-top block of V (published / gathered), M = T V1^H
-// red    [NT/32]          cross-warp reduction scratch
+// ---- PTX helpers -------------------------------------------------------------------
+__device__ __forceinline__ uint32_t su32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+// 16-byte remote store into CTA-rank-mapped shared memory, completion counted on its mbarrier
+__device__ __forceinline__ void st_async(uint32_t raddr, cd v, uint32_t rmbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];"
+               ::"r"(raddr), "d"(v.x), "d"(v.y), "r"(rmbar) : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Bounded wait of the whole CTA on the phase of the given parity.  Only thread 0 polls --
+// polling warps would compete with the computing warps for the shared-memory pipe -- and the
+// block barrier then publishes the completion (and the pushed data) to every thread.  A
+// timeout is recorded in the error word and later waits are skipped.
+__device__ __forceinline__ void cta_wait(uint32_t mbar, uint32_t parity, bool& failed, int* err) {
+  if (threadIdx.x == 0 && !failed) {
+    int it = 0;
+    while (!mbar_test(mbar, parity)) {
+      if (++it >= WAIT_LIMIT) {
+        failed = true;
+        if (err) atomicOr(err, 1);
+        break;
+      }
+    }
+  }
+  __syncthreads();
+}
 
-template <int ROWS>
-__device__ __forceinline__ cd group_sum(cd v, cd* red) {
-  constexpr int W = ROWS < 32 ? ROWS : 32;
+// sum of the C partials part[q*stride] in a fixed order (tree over the ranks, independent loads)
+__device__ __forceinline__ cd sum_ranks(const cd* part, int stride, int C) {
+  cd v[CMAX];
 #pragma unroll
-  for (int off = W / 2; off > 0; off >>= 1) {
+  for (int q = 0; q < CMAX; ++q) v[q] = (q < C) ? part[q * stride] : cmk(0.0, 0.0);
+#pragma unroll
+  for (int w = CMAX / 2; w > 0; w >>= 1)
+#pragma unroll
+    for (int q = 0; q < w; ++q) v[q] = cadd(v[q], v[q + w]);
+  return v[0];
+}
+
+__device__ __forceinline__ cd shfl(cd v, int src) {
+  return cmk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+__device__ __forceinline__ cd warp_sum(cd v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
     v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
     v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
   }
-  if constexpr (ROWS <= 32) {
-    return v;
-  } else {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    __syncthreads();
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    cd s = cmk(0.0, 0.0);
-    if (tid % ROWS == 0) {
+  return v;
+}
+
+// ---- per-CTA shared memory map (complex elements) -------------------------------------
+// S     [(ROWS+1) * n]       this CTA's rows, column-major, ld = ROWS+1
+// rcol  [2][C][2*NB]         column exchange (two parities): pq from each rank, row j from its owner
+// rrs   [C][NB*ksmax]        partials of V^H A received from each rank for my column slice
+// w2s   [NB*ksmax]           my reduced slice
+// rag   [NB*n]               the gathered W2 (all slices)
+// T     [npanels*NB*NB]      compact-WY factors (column-major NB x NB)
+// rv1   [2][NB*NB]           pushed top block V1 of the panel (two parities);  mloc [NB*NB] = T V1^H
+// mbar  [MB_COUNT] u64
+
+// V[r, i] of panel p0 for global row g (unit lower trapezoidal, stored below the diagonal)
+#define VAL_V(g, i, rr) ((g) == p0 + (i) ? cmk(1.0, 0.0) : S[(p0 + (i)) * ldS + (rr)])
+
+// Partial sums W[i, k] = sum over this CTA's rows of conj(V[r, i]) A[r, kb + k] for the panel at
+// p0 (width pw), pushed with st.async to the owner of column slice k / KS.  Threads t in
+// [0, nthr) take (k, half panel) pairs; the rows of the panel's diagonal block (where V is 1 or
+// 0 above its stored part) are handled apart so the bulk loop carries no per-element tests.
+template <int ROWS, int NB>
+__device__ __forceinline__ void partials_push(const cd* S, int ldS, cd* rrs, uint32_t mb_rs, int crank, int ksmax,
+                                              int row0, int m, int p0, int pw, int kb, int nt, int KS, int t,
+                                              int nthr) {
+  const int lo = max(0, p0 - row0), hi = min(ROWS, m - row0);
+  const int mid = min(hi, max(lo, p0 + pw - row0));
+  for (int e = t; e < 2 * nt; e += nthr) {
+    const int k = e % nt, i0 = (e / nt) * (NB / 2);
+    const int iv = min(NB / 2, pw - i0);   // valid panel columns in this half
+    cd acc[NB / 2];
 #pragma unroll
-      for (int w = 0; w < ROWS / 32; ++w) s = cadd(s, red[warp + w]);
+    for (int i = 0; i < NB / 2; ++i) acc[i] = cmk(0.0, 0.0);
+    const cd* Ak = S + (kb + k) * ldS;
+    for (int rr = lo; rr < mid; ++rr) {
+      const int g = row0 + rr;
+      const cd a = Ak[rr];
+#pragma unroll
+      for (int i = 0; i < NB / 2; ++i) {
+        const int ii = i0 + i;
+        if (i < iv && g >= p0 + ii) cfma_cj(acc[i], VAL_V(g, ii, rr), a);
+      }
     }
-    return s;
+    for (int rr = mid; rr < hi; ++rr) {
+      const cd a = Ak[rr];
+#pragma unroll
+      for (int i = 0; i < NB / 2; ++i)
+        if (i < iv) cfma_cj(acc[i], S[(p0 + i0 + i) * ldS + rr], a);
+    }
+    const int so = k / KS, kk = k - so * KS;
+    const uint32_t rm = mapa(mb_rs, so);
+#pragma unroll
+    for (int i = 0; i < NB / 2; ++i)
+      if (i < iv) st_async(mapa(su32(&rrs[crank * NB * ksmax + (i0 + i) + NB * kk]), so), acc[i], rm);
   }
 }
 
-template <int ROWS>
+// Row `rr` of the panel's V (zero above its diagonal block and outside the matrix), in registers.
+template <int NB>
+__device__ __forceinline__ void load_vrow(cd (&v)[NB], const cd* S, int ldS, int rr, int g, int m, int p0, int pw) {
+#pragma unroll
+  for (int i = 0; i < NB; ++i)
+    v[i] = (i < pw && g >= p0 + i && g < m) ? VAL_V(g, i, rr) : cmk(0.0, 0.0);
+}
+
+template <int RPL, int NB>
 __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
+  constexpr int ROWS = 32 * RPL;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* sm = reinterpret_cast<cd*>(smem_raw);
-  constexpr int G = NT / ROWS;   // column groups
-  const int C = P.C, nb = P.nb, ldS = P.ldS;
+  const int C = P.C, ldS = P.ldS, ksmax = P.ksmax;
   const int m = P.p.m, n = P.p.n;
   const int crank = (int)cluster.block_rank();
   const int prob = blockIdx.y;
-  const int tid = threadIdx.x;
-  const int r = tid % ROWS, grp = tid / ROWS;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int row0 = crank * ROWS;
-  const int grow = row0 + r;
+  int* err = P.p.err;
 
   cd* S = sm + P.o_S;
-  cd* bc = sm + P.o_bc;
-  cd* bw = bc + 4;          // w[nb]
-  cd* bt = bw + nb;         // t[nb]
-  cd* sumpq = bt + nb;      // [nb]
-  cd* rowjl = sumpq + nb;   // [nb]
-  cd* wpart = sm + P.o_wpart;
+  cd* rcol = sm + P.o_rcol;
+  cd* rrs = sm + P.o_rrs;
   cd* w2s = sm + P.o_w2s;
+  cd* rag = sm + P.o_rag;
   cd* Tall = sm + P.o_T;
-  cd* v1pub = sm + P.o_v1pub;
-  cd* v1loc = sm + P.o_v1loc;
+  cd* rv1 = sm + P.o_rv1;
   cd* mloc = sm + P.o_mloc;
-  cd* red = sm + P.o_red;
+  cd* bcs = sm + P.o_bc;        // tau, beta, scale of the current column
+  cd* bcw = bcs + 4;            // w_c of the current column
+  cd* tst = sm + P.o_tst;       // tst[jl*NB + c] = t_c (c < jl), tst[jl*NB + jl] = tau_jl
+  uint64_t* mb = reinterpret_cast<uint64_t*>(smem_raw + P.o_mbar);
+  uint32_t mbs[MB_COUNT];
+#pragma unroll
+  for (int k = 0; k < MB_COUNT; ++k) mbs[k] = su32(&mb[k]);
+  uint32_t ph[MB_COUNT];
+#pragma unroll
+  for (int k = 0; k < MB_COUNT; ++k) ph[k] = 0;
+  bool failed = false;
 
-  // ---- load this CTA's rows
-  {
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < MB_COUNT; ++k) mbar_init(mbs[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  {  // ---- load this CTA's rows
     const cd* X = P.p.X + (int64_t)prob * P.p.x_b;
     for (int e = tid; e < ROWS * n; e += NT) {
       int rr = e % ROWS, cc = e / ROWS, g = row0 + rr;
       S[cc * ldS + rr] = (g < m) ? X[(int64_t)g * P.p.x_r + (int64_t)cc * P.p.x_c] : cmk(0.0, 0.0);
     }
   }
-  cluster.sync();
+  cluster.sync();   // mbarriers initialised cluster-wide before any push
 
   // ================================ factorisation ================================
   int sp = 0;
   for (int pi = 0; pi < P.npanels; ++pi) {
-    const int p0 = pi * nb;
-    const int pw = min(nb, n - p0);
-    cd* Tp = Tall + pi * nb * nb;
+    const int p0 = pi * NB;
+    const int pw = min(NB, n - p0);
     for (int jl = 0; jl < pw; ++jl) {
       const int j = p0 + jl;
-      cd* st = sm + P.o_step + sp * P.step_elems;   // pq[nb], rowj[nb]
-      // -- phase A: partial sums over this CTA's rows g > j
-      {
-        cd x = cmk(0.0, 0.0);
-        if (grow > j && grow < m) x = S[j * ldS + r];
-        const int nslots = (pw + G - 1) / G;
-        for (int s = 0; s < nslots; ++s) {
-          int c = grp + G * s;
-          cd v = cmk(0.0, 0.0);
-          if (c < pw && grow > j && grow < m) {
-            cd a = S[(p0 + c) * ldS + r];
-            if (c >= jl) { v = cmul(cconj(x), a); }
-            else         { v = cmul(cconj(a), x); }
+      cd* rb = rcol + sp * (C * 2 * NB);
+      const uint32_t mbc = mbs[MB_COL0 + sp];
+      const int owner = j / ROWS;
+      // -- phase A: partial sums over this CTA's rows g > j, pushed to every CTA
+      cd x[RPL];
+#pragma unroll
+      for (int q = 0; q < RPL; ++q) {
+        int r = lane + 32 * q, g = row0 + r;
+        x[q] = (g > j && g < m) ? S[j * ldS + r] : cmk(0.0, 0.0);
+      }
+      {  // this warp's (at most two) panel columns c0 = warp, c1 = warp + NW, reduced together
+        static_assert(NB <= 2 * NW, "at most two panel columns per warp");
+        const int c0 = warp, c1 = warp + NW;
+        cd a0 = cmk(0.0, 0.0), a1 = cmk(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+          const int r = lane + 32 * q;
+          if (c0 < pw) {
+            const cd a = S[(p0 + c0) * ldS + r];
+            if (c0 >= jl) cfma_cj(a0, x[q], a);   // conj(x) a  (c == jl: |x|^2)
+            else          cfma_cj(a0, a, x[q]);   // conj(a) x  (V^H x for the T column)
           }
-          v = group_sum<ROWS>(v, red);
-          if (r == 0 && c < pw) st[c] = v;
+          if (c1 < pw) {
+            const cd a = S[(p0 + c1) * ldS + r];
+            if (c1 >= jl) cfma_cj(a1, x[q], a);
+            else          cfma_cj(a1, a, x[q]);
+          }
         }
-        if (j >= row0 && j < row0 + ROWS && tid < pw) st[nb + tid] = S[(p0 + tid) * ldS + (j - row0)];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          a0.x += __shfl_xor_sync(0xffffffffu, a0.x, off);
+          a0.y += __shfl_xor_sync(0xffffffffu, a0.y, off);
+          a1.x += __shfl_xor_sync(0xffffffffu, a1.x, off);
+          a1.y += __shfl_xor_sync(0xffffffffu, a1.y, off);
+        }
+        if (lane < C) {
+          const uint32_t rm = mapa(mbc, lane);
+          if (c0 < pw) st_async(mapa(su32(&rb[crank * 2 * NB + c0]), lane), a0, rm);
+          if (c1 < pw) st_async(mapa(su32(&rb[crank * 2 * NB + c1]), lane), a1, rm);
+        }
       }
-      cluster.sync();
-      // -- phase B: gather (fixed order), reflector, w / t, T column
-      if (tid < pw) {
-        cd s = cmk(0.0, 0.0);
-        for (int q = 0; q < C; ++q) s = cadd(s, cluster.map_shared_rank(st, q)[tid]);
-        sumpq[tid] = s;
-      } else if (tid >= 64 && tid < 64 + pw) {
-        int c = tid - 64;
-        rowjl[c] = cluster.map_shared_rank(st, j / ROWS)[nb + c];
+      if (crank == owner && warp == NW - 1 && lane < pw) {
+        const cd v = S[(p0 + lane) * ldS + (j - row0)];
+        for (int q = 0; q < C; ++q) st_async(mapa(su32(&rb[crank * 2 * NB + NB + lane]), q), v, mapa(mbc, q));
       }
-      __syncthreads();
-      if (tid == 0) {
-        cd alpha = rowjl[jl];
-        double xn2 = sumpq[jl].x;
+      if (tid == 0) mbar_expect(mbc, (uint32_t)((C + 1) * pw * sizeof(cd)));
+      cta_wait(mbc, ph[MB_COL0 + sp], failed, err);
+      ph[MB_COL0 + sp] ^= 1;
+      // -- phase B: warp 0 forms the reflector from the gathered sums (local reads only) and
+      // publishes tau / beta / scale, w_c (c > jl) and t_c (c < jl, for T at panel end)
+      if (warp == 0) {
+        cd s = cmk(0.0, 0.0), rj = cmk(0.0, 0.0);
+        if (lane < pw) {
+          s = sum_ranks(rb + lane, 2 * NB, C);
+          rj = rb[owner * 2 * NB + NB + lane];
+        }
+        const cd alpha = shfl(rj, jl);
+        const double xn2 = __shfl_sync(0xffffffffu, s.x, jl);
         cd tau, beta, scale;
         if (xn2 == 0.0 && alpha.y == 0.0) {
           tau = cmk(0.0, 0.0); beta = alpha; scale = cmk(1.0, 0.0);
         } else {
-          double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
-          double b = -copysign(nrm, alpha.x);
-          tau = cmk((b - alpha.x) / b, -alpha.y / b);
+          // tau = (beta - alpha)/beta and scale = 1/(alpha - beta) from two independent
+          // reciprocals, 1/beta and 1/|alpha - beta|^2 (Re(alpha) - beta has no cancellation:
+          // beta carries the opposite sign of Re(alpha))
+          const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+          const double b = -copysign(nrm, alpha.x);
+          const double dr = alpha.x - b;
+          const double ib = 1.0 / b;
+          const double id = 1.0 / (dr * dr + alpha.y * alpha.y);
+          tau = cmk((b - alpha.x) * ib, -alpha.y * ib);
           beta = cmk(b, 0.0);
-          scale = crecip(cmk(alpha.x - b, alpha.y));
+          scale = cmk(dr * id, -alpha.y * id);
         }
-        bc[0] = tau; bc[1] = beta; bc[2] = scale;
+        if (lane > jl && lane < pw) bcw[lane] = cadd(rj, cmul(cconj(scale), s));
+        else if (lane < jl) tst[jl * NB + lane] = cadd(cconj(rj), cmul(scale, s));
+        if (lane == 0) { bcs[0] = tau; bcs[1] = beta; bcs[2] = scale; tst[jl * NB + jl] = tau; }
       }
       __syncthreads();
-      const cd tau = bc[0], beta = bc[1], scale = bc[2];
-      if (tid < pw) {
-        int c = tid;
-        if (c > jl) bw[c] = cadd(rowjl[c], cmul(cconj(scale), sumpq[c]));
-        else if (c < jl) bt[c] = cadd(cconj(rowjl[c]), cmul(scale, sumpq[c]));
-      }
-      // v for this thread's row (read before the column is rewritten)
-      cd vr = cmk(0.0, 0.0);
-      if (grow == j) vr = cmk(1.0, 0.0);
-      else if (grow > j && grow < m) vr = cmul(scale, S[j * ldS + r]);
-      __syncthreads();
-      // T column jl:  T[i, jl] = -tau * sum_{i'=i}^{jl-1} T[i, i'] t[i'],  T[jl, jl] = tau
-      if (tid < jl) {
-        cd s = cmk(0.0, 0.0);
-        for (int i2 = tid; i2 < jl; ++i2) cfma(s, Tp[tid + nb * i2], bt[i2]);
-        Tp[tid + nb * jl] = cmul(cmk(-tau.x, -tau.y), s);
-      } else if (tid == jl) {
-        Tp[jl + nb * jl] = tau;
-      }
-      const bool active = (tau.x != 0.0) || (tau.y != 0.0);
-      if (active) {
-        if (grp == 0) {
-          if (grow == j) S[j * ldS + r] = beta;
-          else if (grow > j && grow < m) S[j * ldS + r] = vr;
+      const cd tau = bcs[0], beta = bcs[1], scale = bcs[2];
+      if ((tau.x != 0.0) || (tau.y != 0.0)) {
+        cd vr[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+          int g = row0 + lane + 32 * q;
+          vr[q] = (g == j) ? cmk(1.0, 0.0) : cmul(scale, x[q]);   // x is 0 above j and in padding
         }
-        if (grow >= j && grow < m) {
-          const cd ctv = cmul(cconj(tau), vr);
-          for (int c = jl + 1 + grp; c < pw; c += G) {
-            cd* a = &S[(p0 + c) * ldS + r];
-            *a = csub(*a, cmul(ctv, bw[c]));
+        const cd ctau = cconj(tau);
+        if (warp == (jl % NW)) {
+#pragma unroll
+          for (int q = 0; q < RPL; ++q) {
+            int r = lane + 32 * q, g = row0 + r;
+            if (g == j) S[j * ldS + r] = beta;
+            else if (g > j && g < m) S[j * ldS + r] = vr[q];
+          }
+        }
+        for (int c = warp; c < pw; c += NW) {
+          if (c > jl) {
+            const cd f = cmul(ctau, bcw[c]);
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) {
+              int r = lane + 32 * q, g = row0 + r;
+              if (g >= j && g < m) {
+                cd* a = &S[(p0 + c) * ldS + r];
+                *a = csub(*a, cmul(f, vr[q]));
+              }
+            }
           }
         }
       }
       __syncthreads();
       sp ^= 1;
     }
+    cd* Tp = Tall + pi * NB * NB;
+    // T (compact WY, zlarft forward/columnwise) from the stashed t vectors, by warp 0 while the
+    // other warps start on the trailing partials: T[0:jl, jl] = -tau_jl T[0:jl, 0:jl] t_jl
+    if (warp == 0) {
+      for (int jl = 0; jl < pw; ++jl) {
+        const cd tj = tst[jl * NB + jl];
+        cd a4[4] = {cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0)};
+#pragma unroll
+        for (int c = 0; c < NB; ++c)   // T[lane, c] = 0 for c < lane, so c starts at 0 harmlessly
+          if (c < jl && lane < jl) cfma(a4[c & 3], Tp[lane + NB * c], tst[jl * NB + c]);
+        const cd acc = cadd(cadd(a4[0], a4[1]), cadd(a4[2], a4[3]));
+        if (lane < NB) Tp[lane + NB * jl] = (lane < jl) ? cmul(cmk(-tj.x, -tj.y), acc) : (lane == jl ? tj : cmk(0.0, 0.0));
+        __syncwarp();
+      }
+    }
 
     // -- trailing update A_t := (I - V T^H V^H) A_t
     const int nt = n - p0 - pw;
     if (nt > 0) {
       const int kb = p0 + pw;
-      for (int e = tid; e < pw * nt; e += NT) {
-        int k = e % nt, i = e / nt;
-        cd acc = cmk(0.0, 0.0);
-        const int lo = max(0, p0 + i - row0);
-        const int hi = min(ROWS, m - row0);
-        for (int rr = lo; rr < hi; ++rr) {
-          cd v = (row0 + rr == p0 + i) ? cmk(1.0, 0.0) : S[(p0 + i) * ldS + rr];
-          cfma_cj(acc, v, S[(kb + k) * ldS + rr]);
-        }
-        wpart[i + nb * k] = acc;
-      }
-      cluster.sync();
       const int KS = (nt + C - 1) / C;
-      const int k0 = crank * KS, k1 = min(nt, k0 + KS);
-      for (int e = tid; e < pw * max(0, k1 - k0); e += NT) {
-        int i = e % pw, k = k0 + e / pw;
+      const int k0 = crank * KS, ks_mine = max(0, min(nt, k0 + KS) - k0);
+      // partials W[i, k] = sum_{my rows} conj(V[r, i]) A[r, k], pushed to the slice owner of k
+      if (warp > 0) partials_push<ROWS, NB>(S, ldS, rrs, mbs[MB_RS], crank, ksmax, row0, m, p0, pw, kb, nt, KS,
+                                            tid - 32, NT - 32);
+      __syncthreads();   // T complete before W2 = T^H W
+      if (tid == 0) mbar_expect(mbs[MB_RS], (uint32_t)(C * pw * ks_mine * sizeof(cd)));
+      cta_wait(mbs[MB_RS], ph[MB_RS], failed, err);
+      ph[MB_RS] ^= 1;
+      for (int e = tid; e < pw * ks_mine; e += NT) {
+        const int i = e % pw, kk = e / pw;
         cd s = cmk(0.0, 0.0);
-        for (int q = 0; q < C; ++q) s = cadd(s, cluster.map_shared_rank(wpart, q)[i + nb * k]);
-        w2s[i + nb * (k - k0)] = s;
+        s = sum_ranks(rrs + i + NB * kk, NB * ksmax, C);
+        w2s[i + NB * kk] = s;
       }
       __syncthreads();
-      // W2 = T^H W, column by column, descending i in place
-      for (int k = k0 + tid; k < k1; k += NT) {
-        cd* wcol = w2s + nb * (k - k0);
-        for (int i = pw - 1; i >= 0; --i) {
-          cd s = cmk(0.0, 0.0);
-          for (int i2 = 0; i2 <= i; ++i2) cfma_cj(s, Tp[i2 + nb * i], wcol[i2]);
-          wcol[i] = s;
-        }
+      // W2 = T^H W on my slice, pushed to every CTA
+      for (int e = tid; e < pw * ks_mine; e += NT) {
+        const int i = e % pw, kk = e / pw;
+        cd s = cmk(0.0, 0.0);
+        for (int i2 = 0; i2 <= i; ++i2) cfma_cj(s, Tp[i2 + NB * i], w2s[i2 + NB * kk]);
+        const uint32_t la = su32(&rag[i + NB * (k0 + kk)]);
+        for (int q = 0; q < C; ++q) st_async(mapa(la, q), s, mapa(mbs[MB_AG], q));
       }
-      cluster.sync();
-      for (int e = tid; e < pw * nt; e += NT) {
-        int i = e % pw, k = e / pw, q = k / KS;
-        wpart[i + nb * k] = cluster.map_shared_rank(w2s, q)[i + nb * (k - q * KS)];
-      }
-      __syncthreads();
-      for (int e = tid; e < ROWS * nt; e += NT) {
-        int rr = e % ROWS, k = e / ROWS;
-        int g = row0 + rr;
-        if (g < p0 || g >= m) continue;
-        cd acc = cmk(0.0, 0.0);
-        const int imax = min(pw - 1, g - p0);
-        for (int i = 0; i <= imax; ++i) {
-          cd v = (g == p0 + i) ? cmk(1.0, 0.0) : S[(p0 + i) * ldS + rr];
-          cfma(acc, v, wpart[i + nb * k]);
+      if (tid == 0) mbar_expect(mbs[MB_AG], (uint32_t)(pw * nt * sizeof(cd)));
+      cta_wait(mbs[MB_AG], ph[MB_AG], failed, err);
+      ph[MB_AG] ^= 1;
+      // A[r, k] -= sum_i V[r, i] W2[i, k]: thread = (row, column group), its V row in registers
+      {
+        constexpr int G = NT / ROWS;
+        const int rr = tid % ROWS, grp = tid / ROWS, g = row0 + rr;
+        if (g >= p0 && g < m) {
+          cd v[NB];
+          load_vrow<NB>(v, S, ldS, rr, g, m, p0, pw);
+          for (int k = grp; k < nt; k += G) {
+            cd acc = cmk(0.0, 0.0);
+#pragma unroll
+            for (int i = 0; i < NB; ++i)
+              if (i < pw) cfma(acc, v[i], rag[i + NB * k]);
+            cd* a = &S[(kb + k) * ldS + rr];
+            *a = csub(*a, acc);
+          }
         }
-        cd* a = &S[(kb + k) * ldS + rr];
-        *a = csub(*a, acc);
       }
       __syncthreads();
     }
@@ -278,179 +432,171 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
   // rows above each column's panel start are zero in the partially formed Q
   for (int e = tid; e < ROWS * n; e += NT) {
     int rr = e % ROWS, k = e / ROWS, g = row0 + rr;
-    if (g < (k / nb) * nb) S[k * ldS + rr] = cmk(0.0, 0.0);
+    if (g < (k / NB) * NB) S[k * ldS + rr] = cmk(0.0, 0.0);
   }
   __syncthreads();
 
   // ================================ Q formation ==================================
+  int vp = 0;
   for (int pi = P.npanels - 1; pi >= 0; --pi) {
-    const int p0 = pi * nb;
-    const int pw = min(nb, n - p0);
+    const int p0 = pi * NB;
+    const int pw = min(NB, n - p0);
     const int nt = n - p0 - pw, kb = p0 + pw;
-    const cd* Tp = Tall + pi * nb * nb;
-    // partials V^H Q_trail and the published top block V1[c, i] = V[p0 + c, i]
-    for (int e = tid; e < pw * nt; e += NT) {
-      int k = e % nt, i = e / nt;
-      cd acc = cmk(0.0, 0.0);
-      const int lo = max(0, p0 + i - row0);
-      const int hi = min(ROWS, m - row0);
-      for (int rr = lo; rr < hi; ++rr) {
-        cd v = (row0 + rr == p0 + i) ? cmk(1.0, 0.0) : S[(p0 + i) * ldS + rr];
-        cfma_cj(acc, v, S[(kb + k) * ldS + rr]);
-      }
-      wpart[i + nb * k] = acc;
-    }
+    const cd* Tp = Tall + pi * NB * NB;
+    const int KS = nt > 0 ? (nt + C - 1) / C : 1;
+    const int k0 = crank * KS, ks_mine = max(0, min(nt, k0 + KS) - k0);
+    cd* v1 = rv1 + vp * NB * NB;
+    const uint32_t mbv = mbs[MB_V10 + vp];
+    // partials of V^H Q_trail pushed to slice owners; top block V1 pushed to every CTA
+    if (nt > 0) partials_push<ROWS, NB>(S, ldS, rrs, mbs[MB_RS], crank, ksmax, row0, m, p0, pw, kb, nt, KS, tid, NT);
     for (int e = tid; e < pw * pw; e += NT) {
-      int c = e % pw, i = e / pw, g = p0 + c;
+      const int c = e % pw, i = e / pw, g = p0 + c;
       if (g >= row0 && g < row0 + ROWS) {
-        cd v = (c == i) ? cmk(1.0, 0.0) : (c > i ? S[(p0 + i) * ldS + (g - row0)] : cmk(0.0, 0.0));
-        v1pub[c + nb * i] = v;
+        const cd v = (c == i) ? cmk(1.0, 0.0) : (c > i ? S[(p0 + i) * ldS + (g - row0)] : cmk(0.0, 0.0));
+        const uint32_t la = su32(&v1[c + NB * i]);
+        for (int q = 0; q < C; ++q) st_async(mapa(la, q), v, mapa(mbv, q));
       }
     }
-    cluster.sync();
-    const int KS = (nt + C - 1) / C;
-    const int k0 = crank * KS, k1 = min(nt, k0 + KS);
-    for (int e = tid; e < pw * max(0, k1 - k0); e += NT) {
-      int i = e % pw, k = k0 + e / pw;
-      cd s = cmk(0.0, 0.0);
-      for (int q = 0; q < C; ++q) s = cadd(s, cluster.map_shared_rank(wpart, q)[i + nb * k]);
-      w2s[i + nb * (k - k0)] = s;
-    }
-    for (int e = tid; e < pw * pw; e += NT) {
-      int c = e % pw, i = e / pw;
-      v1loc[c + nb * i] = cluster.map_shared_rank(v1pub, (p0 + c) / ROWS)[c + nb * i];
-    }
-    __syncthreads();
-    // W2 = T W, ascending i in place
-    for (int k = k0 + tid; k < k1; k += NT) {
-      cd* wcol = w2s + nb * (k - k0);
-      for (int i = 0; i < pw; ++i) {
+    if (nt > 0) {
+      if (tid == 0) mbar_expect(mbs[MB_RS], (uint32_t)(C * pw * ks_mine * sizeof(cd)));
+      cta_wait(mbs[MB_RS], ph[MB_RS], failed, err);
+      ph[MB_RS] ^= 1;
+      for (int e = tid; e < pw * ks_mine; e += NT) {
+        const int i = e % pw, kk = e / pw;
         cd s = cmk(0.0, 0.0);
-        for (int i2 = i; i2 < pw; ++i2) cfma(s, Tp[i + nb * i2], wcol[i2]);
-        wcol[i] = s;
+        s = sum_ranks(rrs + i + NB * kk, NB * ksmax, C);
+        w2s[i + NB * kk] = s;
       }
     }
-    // M = T V1^H  (M[i, c] = sum_{i2 >= i} T[i, i2] conj(V1[c, i2]))
+    // M = T V1^H  (M[i, c] = sum_{i2 = i..c} T[i, i2] conj(V1[c, i2])), read before any AG push
+    if (tid == 0) mbar_expect(mbv, (uint32_t)(pw * pw * sizeof(cd)));
+    cta_wait(mbv, ph[MB_V10 + vp], failed, err);
+    ph[MB_V10 + vp] ^= 1;
     for (int e = tid; e < pw * pw; e += NT) {
-      int i = e % pw, c = e / pw;
+      const int i = e % pw, c = e / pw;
       cd s = cmk(0.0, 0.0);
-      for (int i2 = i; i2 <= c && i2 < pw; ++i2) cfma(s, Tp[i + nb * i2], cconj(v1loc[c + nb * i2]));
-      mloc[i + nb * c] = s;
-    }
-    cluster.sync();
-    for (int e = tid; e < pw * nt; e += NT) {
-      int i = e % pw, k = e / pw, q = k / KS;
-      wpart[i + nb * k] = cluster.map_shared_rank(w2s, q)[i + nb * (k - q * KS)];
+      for (int i2 = i; i2 <= c; ++i2) cfma(s, Tp[i + NB * i2], cconj(v1[c + NB * i2]));
+      mloc[i + NB * c] = s;
     }
     __syncthreads();
-    // Q_trail -= V W2
-    for (int e = tid; e < ROWS * nt; e += NT) {
-      int rr = e % ROWS, k = e / ROWS, g = row0 + rr;
-      if (g < p0 || g >= m) continue;
-      cd acc = cmk(0.0, 0.0);
-      const int imax = min(pw - 1, g - p0);
-      for (int i = 0; i <= imax; ++i) {
-        cd v = (g == p0 + i) ? cmk(1.0, 0.0) : S[(p0 + i) * ldS + rr];
-        cfma(acc, v, wpart[i + nb * k]);
+    if (nt > 0) {
+      // W2 = T W on my slice, pushed to every CTA
+      for (int e = tid; e < pw * ks_mine; e += NT) {
+        const int i = e % pw, kk = e / pw;
+        cd s = cmk(0.0, 0.0);
+        for (int i2 = i; i2 < pw; ++i2) cfma(s, Tp[i + NB * i2], w2s[i2 + NB * kk]);
+        const uint32_t la = su32(&rag[i + NB * (k0 + kk)]);
+        for (int q = 0; q < C; ++q) st_async(mapa(la, q), s, mapa(mbs[MB_AG], q));
       }
-      cd* a = &S[(kb + k) * ldS + rr];
-      *a = csub(*a, acc);
+      if (tid == 0) mbar_expect(mbs[MB_AG], (uint32_t)(pw * nt * sizeof(cd)));
+      cta_wait(mbs[MB_AG], ph[MB_AG], failed, err);
+      ph[MB_AG] ^= 1;
     }
-    __syncthreads();
-    // panel block: Q[g, p0 + c] = delta(g, p0 + c) - sum_i V[g, i] M[i, c]
-    cd qv[(NT / 8 + 1)];   // upper bound on columns per thread (pw / G + 1 <= 33)
-    int cnt = 0;
-    const int g = grow;
-    for (int c = grp; c < pw; c += G) {
-      cd acc = cmk(0.0, 0.0);
+    // Q_trail -= V W2 and the panel block Q[g, p0 + c] = delta(g, p0 + c) - sum_i V[g, i] M[i, c];
+    // thread = (row, column group) with its V row in registers, read before the panel is rewritten
+    {
+      constexpr int G = NT / ROWS;
+      const int rr = tid % ROWS, grp = tid / ROWS, g = row0 + rr;
+      cd v[NB];
+      load_vrow<NB>(v, S, ldS, rr, g, m, p0, pw);
+      __syncthreads();
       if (g >= p0 && g < m) {
-        const int imax = min(pw - 1, g - p0);
-        for (int i = 0; i <= imax; ++i) {
-          cd v = (g == p0 + i) ? cmk(1.0, 0.0) : S[(p0 + i) * ldS + r];
-          cfma(acc, v, mloc[i + nb * c]);
+        for (int k = grp; k < nt; k += G) {
+          cd acc = cmk(0.0, 0.0);
+#pragma unroll
+          for (int i = 0; i < NB; ++i)
+              if (i < pw) cfma(acc, v[i], rag[i + NB * k]);
+          cd* a = &S[(kb + k) * ldS + rr];
+          *a = csub(*a, acc);
         }
       }
-      cd d = (g == p0 + c) ? cmk(1.0, 0.0) : cmk(0.0, 0.0);
-      qv[cnt++] = csub(d, acc);
+      for (int c = grp; c < pw; c += G) {
+        cd acc = cmk(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+          if (i < pw) cfma(acc, v[i], mloc[i + NB * c]);
+        S[(p0 + c) * ldS + rr] = csub((g == p0 + c) ? cmk(1.0, 0.0) : cmk(0.0, 0.0), acc);
+      }
     }
     __syncthreads();
-    cnt = 0;
-    for (int c = grp; c < pw; c += G) S[(p0 + c) * ldS + r] = qv[cnt++];
-    __syncthreads();
+    vp ^= 1;
   }
 
-  // ---- write Q (this CTA's rows)
-  {
+  {  // ---- write Q (this CTA's rows)
     cd* Q = P.p.Q + (int64_t)prob * P.p.q_b;
     for (int e = tid; e < ROWS * n; e += NT) {
       int rr = e % ROWS, cc = e / ROWS, g = row0 + rr;
       if (g < m) Q[(int64_t)g * P.p.q_r + (int64_t)cc * P.p.q_c] = S[cc * ldS + rr];
     }
   }
-  // keep this CTA's shared memory alive until every peer has finished its DSMEM reads
+  // no CTA leaves while a peer may still address its shared memory
   cluster.sync();
 }
+#undef VAL_V
 
 typedef void (*QrKernel)(QrParams);
 
-QrKernel kernel_for(int rows) {
-  switch (rows) {
-    case 8: return qr_kernel<8>;
-    case 16: return qr_kernel<16>;
-    case 32: return qr_kernel<32>;
-    case 64: return qr_kernel<64>;
-    case 128: return qr_kernel<128>;
-    case 256: return qr_kernel<256>;
+template <int NB>
+QrKernel kernel_rpl(int rpl) {
+  switch (rpl) {
+    case 1: return qr_kernel<1, NB>;
+    case 2: return qr_kernel<2, NB>;
+    case 4: return qr_kernel<4, NB>;
     default: return nullptr;
   }
 }
 
-int next_pow2(int v) {
-  int p = 8;
-  while (p < v) p <<= 1;
-  return p;
+QrKernel kernel_for(int rpl, int nb) {
+  if (nb == 16) return kernel_rpl<16>(rpl);
+  if (nb == 8) return kernel_rpl<8>(rpl);
+  if (nb == 4) return kernel_rpl<4>(rpl);
+  return nullptr;
 }
 
-size_t layout(QrParams& P, int m, int n, int C, int rows, int nb) {
-  P.C = C; P.rows = rows; P.nb = nb;
+size_t layout(QrParams& P, int n, int C, int rows, int nb) {
+  P.C = C;
   P.npanels = (n + nb - 1) / nb;
   P.ldS = rows + 1;
-  P.step_elems = 2 * nb;
-  P.w2s_cols = (n + C - 1) / C;
+  P.ksmax = (n + C - 1) / C;
   int o = 0;
-  P.o_S = o;      o += P.ldS * n;
-  P.o_step = o;   o += 2 * P.step_elems;
-  P.o_bc = o;     o += 4 + 4 * nb;
-  P.o_wpart = o;  o += nb * n;
-  P.o_w2s = o;    o += nb * P.w2s_cols;
-  P.o_T = o;      o += P.npanels * nb * nb;
-  P.o_v1pub = o;  o += nb * nb;
-  P.o_v1loc = o;  o += nb * nb;
-  P.o_mloc = o;   o += nb * nb;
-  P.o_red = o;    o += NT / 32;
-  (void)m;
-  return (size_t)o * sizeof(cd);
+  P.o_S = o;     o += P.ldS * n;
+  P.o_rcol = o;  o += 2 * C * 2 * nb;
+  P.o_rrs = o;   o += C * nb * P.ksmax;
+  P.o_w2s = o;   o += nb * P.ksmax;
+  P.o_rag = o;   o += nb * n;
+  P.o_T = o;     o += P.npanels * nb * nb;
+  P.o_rv1 = o;   o += 2 * nb * nb;
+  P.o_mloc = o;  o += nb * nb;
+  P.o_bc = o;    o += 4 + nb;        // tau, beta, scale, pad; w[nb]
+  P.o_tst = o;   o += nb * nb;       // t vectors (and tau) of the panel's columns
+  P.o_mbar = o * (int)sizeof(cd);
+  return (size_t)P.o_mbar + MB_COUNT * sizeof(uint64_t);
 }
 
-// Pick (cluster size, rows per CTA, panel width): the smallest cluster whose CTAs hold at
-// most 64 rows (fewer barriers per column vs. more rows per CTA), then the widest panel that
-// fits in shared memory.  MPSB_QR_CLUSTER overrides the cluster size (tuning).
-bool choose(int m, int n, QrParams& P, size_t& smem) {
-  static const int env_c = [] {
-    const char* s = getenv("MPSB_QR_CLUSTER");
+struct Choice {
+  int C = 0, rpl = 0, nb = 0;
+  size_t smem = 0;
+};
+
+// Cluster of C = ceil(m / (32 rpl)) CTAs, at most 16: prefer 1 row per lane (measured: the
+// per-CTA work, not the exchange, sets the time), then 2, then 4; the widest panel that fits.
+// MPSB_QR_RPL overrides the rows per lane (tuning).
+bool choose(int m, int n, Choice& ch) {
+  static const int env_rpl = [] {
+    const char* s = getenv("MPSB_QR_RPL");
     return s ? atoi(s) : 0;
   }();
-  const int cands[] = {1, 2, 4, 8, 16};
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int C : cands) {
-      if (env_c > 0 && C != env_c) continue;
-      int rows = next_pow2((m + C - 1) / C);
-      if (rows > 256) continue;
-      if (pass == 0 && rows > 64 && C < 16 && env_c == 0) continue;
-      for (int nb : {32, 16, 8, 4}) {
-        if (nb > n && nb > 4) continue;
-        size_t b = layout(P, m, n, C, rows, nb);
-        if (b <= SMEM_LIMIT) { smem = b; return true; }
+  QrParams P;
+  for (int rpl : {1, 2, 4}) {
+    if (env_rpl > 0 && rpl != env_rpl) continue;
+    const int rows = 32 * rpl;
+    const int C = (m + rows - 1) / rows;
+    if (C > CMAX) continue;
+    for (int nb : {16, 8, 4}) {
+      size_t b = layout(P, n, C, rows, nb);
+      if (b <= SMEM_LIMIT) {
+        ch.C = C; ch.rpl = rpl; ch.nb = nb; ch.smem = b;
+        return true;
       }
     }
   }
@@ -460,39 +606,38 @@ bool choose(int m, int n, QrParams& P, size_t& smem) {
 }  // namespace
 
 bool qr_supported(int m, int n) {
-  QrParams P;
-  size_t smem;
-  return m >= n && n >= 1 && choose(m, n, P, smem);
+  Choice ch;
+  return m >= n && n >= 1 && choose(m, n, ch);
 }
 
 int qr_launch(const QrProblem& p, cudaStream_t s) {
   if (p.m < p.n || p.n < 1 || p.batch < 1) return MPSB_ERR_DIMENSION;
   if (p.batch > 65535) return MPSB_ERR_UNSUPPORTED;
-  QrParams P;
-  size_t smem;
-  if (!choose(p.m, p.n, P, smem)) {
+  Choice ch;
+  if (!choose(p.m, p.n, ch)) {
     set_last_message("QR of a %d x %d matrix exceeds the cluster shared-memory capacity", p.m, p.n);
     return MPSB_ERR_UNSUPPORTED;
   }
+  QrParams P;
+  layout(P, p.n, ch.C, 32 * ch.rpl, ch.nb);
   P.p = p;
-  QrKernel fn = kernel_for(P.rows);
+  QrKernel fn = kernel_for(ch.rpl, ch.nb);
   if (!fn) return MPSB_ERR_UNSUPPORTED;
-  static bool attr_done[9] = {false};
-  int key = 0;
-  while ((8 << key) < P.rows) ++key;
-  if (!attr_done[key]) {
+  static bool attr_done[3][8] = {};
+  bool& done = attr_done[ch.nb == 16 ? 2 : (ch.nb == 8 ? 1 : 0)][ch.rpl];
+  if (!done) {
     MPSB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT));
     MPSB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    attr_done[key] = true;
+    done = true;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(P.C, p.batch, 1);
+  cfg.gridDim = dim3(ch.C, p.batch, 1);
   cfg.blockDim = dim3(NT, 1, 1);
-  cfg.dynamicSmemBytes = smem;
+  cfg.dynamicSmemBytes = ch.smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = P.C;
+  attr[0].val.clusterDim.x = ch.C;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
