@@ -5,12 +5,13 @@
 // (m, k[, batch]) element-stride triple, so reference transposes ('), (.') and the
 // reshape/permutedims chains cost no copies.
 //
-// Tiling (FP64 pipe, DFMA): 64x64 complex C tile per 256-thread CTA, each thread owns a
-// 4x4 complex micro-tile strided by 16 (so A fragments are read as 16 consecutive complex,
-// B fragments are warp broadcasts), K staged 16 complex deep through a two-stage cp.async
-// ring in dynamic shared memory (2 x 2 x 16 x 65 x 16 B = 66.5 KB).  Skinny problems split
-// K across CTAs into a workspace that a second kernel sums in a fixed order, so results
-// are bitwise reproducible run to run.
+// Tiling (FP64 tensor path, DMMA): 64x64 complex C tile per 128-thread CTA; each warp owns
+// 32x32 complex as 4x4 blocks of 8x8 and issues mma.sync.m8n8k4.f64 -- four real products
+// per complex k4 step (Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br) -- with every fragment
+// element loaded as one 16-byte (re, im) pair from shared memory.  K is staged 16 complex
+// deep through a three-stage cp.async ring (3 x 2 x 16 x 65 x 16 B = 99.8 KB, two CTAs per
+// SM).  Skinny problems split K across CTAs into a workspace that a second kernel sums in a
+// fixed order, so results are bitwise reproducible run to run.
 #include "common.cuh"
 #include "workspace.cuh"
 
@@ -18,10 +19,10 @@ namespace mpsb {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, NT = 256, PAD = 1;
+constexpr int BM = 64, BN = 64, BK = 16, NT = 128, PAD = 1, STAGES = 3;
 constexpr int LDA_S = BM + PAD, LDB_S = BN + PAD;
 constexpr size_t STAGE_ELEMS = size_t(BK) * LDA_S + size_t(BK) * LDB_S;
-constexpr size_t SMEM_BYTES = 2 * STAGE_ELEMS * sizeof(cd);
+constexpr size_t SMEM_BYTES = STAGES * STAGE_ELEMS * sizeof(cd);
 
 struct GemmParams {
   Gemm g;
@@ -38,6 +39,13 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pr
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// D (8x8, 2 per lane) += A (8x4 row, 1 per lane) * B (4x8 col, 1 per lane)
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
 
 template <bool A_MCONTIG, bool B_KCONTIG>
 __device__ __forceinline__ void load_tile(cd* As, cd* Bs, const cd* A, const cd* B, const Gemm& g,
@@ -71,7 +79,7 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(GemmParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* smem = reinterpret_cast<cd*>(smem_raw);
   const Gemm& g = P.g;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tiles_m = (g.M + BM - 1) / BM;
   const int m0 = (blockIdx.x % tiles_m) * BM;
   const int n0 = (blockIdx.x / tiles_m) * BN;
@@ -83,63 +91,81 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(GemmParams P) {
   const int KT = (g.K + BK - 1) / BK;
   const int kt0 = split * P.kt_per_split;
   const int kt1 = min(KT, kt0 + P.kt_per_split);
+  const int nkt = max(0, kt1 - kt0);
 
-  const int tm = tid % 16, tn = tid / 16;
-  cd acc[4][4];
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  const int fr = lane >> 2, fk = lane & 3;   // fragment row/col within an 8x4 (or 4x8) block
+  double cr[4][4][2], ci[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = cmk(0.0, 0.0);
+    for (int j = 0; j < 4; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
 
-  if (kt0 < kt1) {
-    load_tile<A_MCONTIG, B_KCONTIG>(smem, smem + BK * LDA_S, A, B, g, m0, n0, kt0 * BK, tid);
-    cp_async_commit();
-    for (int kt = kt0; kt < kt1; ++kt) {
-      const int st = (kt - kt0) & 1;
-      if (kt + 1 < kt1) {
-        cd* nxt = smem + (st ^ 1) * STAGE_ELEMS;
-        load_tile<A_MCONTIG, B_KCONTIG>(nxt, nxt + BK * LDA_S, A, B, g, m0, n0, (kt + 1) * BK, tid);
-        cp_async_commit();
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-      __syncthreads();
-      const cd* As = smem + st * STAGE_ELEMS;
-      const cd* Bs = As + BK * LDA_S;
-#pragma unroll 4
-      for (int k = 0; k < BK; ++k) {
-        cd a[4], bb[4];
+  // prologue: STAGES-1 tiles in flight
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          a[i] = As[k * LDA_S + tm + 16 * i];
-          if (CONJA) a[i].y = -a[i].y;
-        }
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nkt) {
+      cd* st = smem + s * STAGE_ELEMS;
+      load_tile<A_MCONTIG, B_KCONTIG>(st, st + BK * LDA_S, A, B, g, m0, n0, (kt0 + s) * BK, tid);
+    }
+    cp_async_commit();
+  }
+  for (int t = 0; t < nkt; ++t) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {  // refill the stage consumed two iterations ago
+      const int tn = t + STAGES - 1;
+      if (tn < nkt) {
+        cd* st = smem + (tn % STAGES) * STAGE_ELEMS;
+        load_tile<A_MCONTIG, B_KCONTIG>(st, st + BK * LDA_S, A, B, g, m0, n0, (kt0 + tn) * BK, tid);
+      }
+      cp_async_commit();
+    }
+    const cd* As = smem + (t % STAGES) * STAGE_ELEMS;
+    const cd* Bs = As + BK * LDA_S;
+#pragma unroll
+    for (int k4 = 0; k4 < BK; k4 += 4) {
+      double ar[4], ai[4], nai[4], br[4], bi[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const cd a = As[(k4 + fk) * LDA_S + wm + 8 * i + fr];
+        ar[i] = a.x;
+        ai[i] = CONJA ? -a.y : a.y;
+        nai[i] = -ai[i];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const cd bb = Bs[(k4 + fk) * LDB_S + wn + 8 * j + fr];
+        br[j] = bb.x;
+        bi[j] = CONJB ? -bb.y : bb.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          bb[j] = Bs[k * LDB_S + tn + 16 * j];
-          if (CONJB) bb[j].y = -bb[j].y;
+          dmma(cr[i][j], ar[i], br[j]);
+          dmma(ci[i][j], ar[i], bi[j]);
+          dmma(cr[i][j], nai[i], bi[j]);
+          dmma(ci[i][j], ai[i], br[j]);
         }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], bb[j]);
-      }
-      __syncthreads();
     }
   }
+  cp_async_wait<0>();
 
+  // accumulator (i, j, e): row wm + 8i + fr, column wn + 8j + 2fk + e
   if (P.splits > 1) {
     cd* W = P.ws + ((int64_t)split * g.batch + b) * (int64_t)g.M * g.N;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      int m = m0 + tm + 16 * i;
+      const int m = m0 + wm + 8 * i + fr;
       if (m >= g.M) continue;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        int n = n0 + tn + 16 * j;
-        if (n < g.N) W[(int64_t)n * g.M + m] = acc[i][j];
-      }
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int n = n0 + wn + 8 * j + 2 * fk + e;
+          if (n < g.N) W[(int64_t)n * g.M + m] = cmk(cr[i][j][e], ci[i][j][e]);
+        }
     }
     return;
   }
@@ -147,17 +173,19 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(GemmParams P) {
   const bool use_beta = (g.beta.x != 0.0) || (g.beta.y != 0.0);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    int m = m0 + tm + 16 * i;
+    const int m = m0 + wm + 8 * i + fr;
     if (m >= g.M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int n = n0 + tn + 16 * j;
-      if (n >= g.N) continue;
-      cd* c = C + (int64_t)m * g.c_m + (int64_t)n * g.c_n;
-      cd v = cmul(g.alpha, acc[i][j]);
-      if (use_beta) v = cadd(v, cmul(g.beta, *c));
-      *c = v;
-    }
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int n = n0 + wn + 8 * j + 2 * fk + e;
+        if (n >= g.N) continue;
+        cd* c = C + (int64_t)m * g.c_m + (int64_t)n * g.c_n;
+        cd v = cmul(g.alpha, cmk(cr[i][j][e], ci[i][j][e]));
+        if (use_beta) v = cadd(v, cmul(g.beta, *c));
+        *c = v;
+      }
   }
 }
 
