@@ -6,12 +6,13 @@
 // reshape/permutedims chains cost no copies.
 //
 // Tiling (FP64 tensor path, DMMA): 64x64 complex C tile per 128-thread CTA; each warp owns
-// 32x32 complex as 4x4 blocks of 8x8 and issues mma.sync.m8n8k4.f64 -- four real products
-// per complex k4 step (Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br) -- with every fragment
+// 32x32 complex as 2x4 blocks of 16x8 and issues mma.sync.m16n8k8.f64 -- four real products
+// per complex k8 step (Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br) -- with every fragment
 // element loaded as one 16-byte (re, im) pair from shared memory.  K is staged 16 complex
-// deep through a three-stage cp.async ring (3 x 2 x 16 x 65 x 16 B = 99.8 KB, two CTAs per
-// SM).  Skinny problems split K across CTAs into a workspace that a second kernel sums in a
-// fixed order, so results are bitwise reproducible run to run.
+// deep through a three-stage cp.async ring (3 x 2 x 16 x 66 x 16 B = 101 KB, two CTAs per
+// SM); the row pitch of 66 elements puts the eight 16-byte fragment loads of a quarter warp
+// in eight distinct bank groups.  Skinny problems split K across CTAs into a workspace that a
+// second kernel sums in a fixed order, so results are bitwise reproducible run to run.
 #include "common.cuh"
 #include "workspace.cuh"
 
@@ -19,7 +20,7 @@ namespace mpsb {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, NT = 128, PAD = 1, STAGES = 3;
+constexpr int BM = 64, BN = 64, BK = 16, NT = 128, PAD = 2, STAGES = 3;
 constexpr int LDA_S = BM + PAD, LDB_S = BN + PAD;
 constexpr size_t STAGE_ELEMS = size_t(BK) * LDA_S + size_t(BK) * LDB_S;
 constexpr size_t SMEM_BYTES = STAGES * STAGE_ELEMS * sizeof(cd);
@@ -40,11 +41,14 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-// D (8x8, 2 per lane) += A (8x4 row, 1 per lane) * B (4x8 col, 1 per lane)
-__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
+// D (16x8, 4 per lane) += A (16x8 row, 4 per lane) * B (8x8 col, 2 per lane).  Lane l holds
+// g = l/4, t = l%4: A (g, t), (g+8, t), (g, t+4), (g+8, t+4); B (t, g), (t+4, g);
+// D (g, 2t), (g, 2t+1), (g+8, 2t), (g+8, 2t+1).
+__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 template <bool A_MCONTIG, bool B_KCONTIG>
@@ -94,12 +98,15 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(GemmParams P) {
   const int nkt = max(0, kt1 - kt0);
 
   const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-  const int fr = lane >> 2, fk = lane & 3;   // fragment row/col within an 8x4 (or 4x8) block
-  double cr[4][4][2], ci[4][4][2];
+  const int fg = lane >> 2, ft = lane & 3;   // fragment group / thread-in-group
+  // accumulators: 2 (16-row) x 4 (8-column) blocks of the warp's 32x32 tile
+  double cr[2][4][4], ci[2][4][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) cr[i][j][e] = ci[i][j][e] = 0.0;
 
   // prologue: STAGES-1 tiles in flight
 #pragma unroll
@@ -124,69 +131,78 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(GemmParams P) {
     const cd* As = smem + (t % STAGES) * STAGE_ELEMS;
     const cd* Bs = As + BK * LDA_S;
 #pragma unroll
-    for (int k4 = 0; k4 < BK; k4 += 4) {
-      double ar[4], ai[4], nai[4], br[4], bi[4];
+    for (int k8 = 0; k8 < BK; k8 += 8) {
+      double ar[2][4], ai[2][4], nai[2][4], br[4][2], bi[4][2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const cd a = As[(k4 + fk) * LDA_S + wm + 8 * i + fr];
-        ar[i] = a.x;
-        ai[i] = CONJA ? -a.y : a.y;
-        nai[i] = -ai[i];
-      }
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const cd bb = Bs[(k4 + fk) * LDB_S + wn + 8 * j + fr];
-        br[j] = bb.x;
-        bi[j] = CONJB ? -bb.y : bb.y;
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          dmma(cr[i][j], ar[i], br[j]);
-          dmma(ci[i][j], ar[i], bi[j]);
-          dmma(cr[i][j], nai[i], bi[j]);
-          dmma(ci[i][j], ai[i], br[j]);
+        for (int e = 0; e < 4; ++e) {
+          const cd a = As[(k8 + ft + 4 * (e >> 1)) * LDA_S + wm + 16 * i + 8 * (e & 1) + fg];
+          ar[i][e] = a.x;
+          ai[i][e] = CONJA ? -a.y : a.y;
+          nai[i][e] = -ai[i][e];
         }
-    }
-  }
-  cp_async_wait<0>();
-
-  // accumulator (i, j, e): row wm + 8i + fr, column wn + 8j + 2fk + e
-  if (P.splits > 1) {
-    cd* W = P.ws + ((int64_t)split * g.batch + b) * (int64_t)g.M * g.N;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int m = m0 + wm + 8 * i + fr;
-      if (m >= g.M) continue;
 #pragma unroll
       for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          const int n = n0 + wn + 8 * j + 2 * fk + e;
-          if (n < g.N) W[(int64_t)n * g.M + m] = cmk(cr[i][j][e], ci[i][j][e]);
+          const cd bb = Bs[(k8 + ft + 4 * e) * LDB_S + wn + 8 * j + fg];
+          br[j][e] = bb.x;
+          bi[j][e] = CONJB ? -bb.y : bb.y;
         }
+      // Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br, term-major so one accumulator's two
+      // products sit eight issues apart
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma16(cr[i][j], ar[i], br[j]);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma16(ci[i][j], ar[i], bi[j]);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma16(cr[i][j], nai[i], bi[j]);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma16(ci[i][j], ai[i], br[j]);
     }
+  }
+  cp_async_wait<0>();
+
+  // accumulator (i, j, e): row wm + 16i + 8(e/2) + fg, column wn + 8j + 2ft + e%2
+  if (P.splits > 1) {
+    cd* W = P.ws + ((int64_t)split * g.batch + b) * (int64_t)g.M * g.N;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int m = m0 + wm + 16 * i + 8 * (e >> 1) + fg;
+          const int n = n0 + wn + 8 * j + 2 * ft + (e & 1);
+          if (m < g.M && n < g.N) W[(int64_t)n * g.M + m] = cmk(cr[i][j][e], ci[i][j][e]);
+        }
     return;
   }
   cd* C = g.C + (int64_t)b * g.c_b;
   const bool use_beta = (g.beta.x != 0.0) || (g.beta.y != 0.0);
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int m = m0 + wm + 8 * i + fr;
-    if (m >= g.M) continue;
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int n = n0 + wn + 8 * j + 2 * fk + e;
-        if (n >= g.N) continue;
+      for (int e = 0; e < 4; ++e) {
+        const int m = m0 + wm + 16 * i + 8 * (e >> 1) + fg;
+        const int n = n0 + wn + 8 * j + 2 * ft + (e & 1);
+        if (m >= g.M || n >= g.N) continue;
         cd* c = C + (int64_t)m * g.c_m + (int64_t)n * g.c_n;
         cd v = cmul(g.alpha, cmk(cr[i][j][e], ci[i][j][e]));
         if (use_beta) v = cadd(v, cmul(g.beta, *c));
         *c = v;
       }
-  }
 }
 
 __global__ void splitk_reduce_kernel(Gemm g, int splits, const cd* __restrict__ ws) {
