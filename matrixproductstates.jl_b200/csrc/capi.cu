@@ -145,6 +145,7 @@ int mpsb_ctx_destroy(mpsb_ctx* ctx) {
   for (auto& b : ctx->ws.named)
     if (b.p) cudaFree(b.p);
   if (ctx->ws.splitk.p) cudaFree(ctx->ws.splitk.p);
+  if (ctx->ws.qr.p) cudaFree(ctx->ws.qr.p);
   cudaFree(ctx->d_scalars);
   cudaFreeHost(ctx->h_scalars);
   cudaStreamDestroy(ctx->own_stream);
@@ -600,8 +601,7 @@ int mpsb_op_qr(mpsb_ctx* ctx, const void* X, void* Q, void* R, int m, int n) {
   p.Q = DW(Q); p.q_r = 1; p.q_c = m;
   if (R) { p.R = DW(R); p.r_r = 1; p.r_c = n; }
   p.err = ctx->err();
-  count_launch(&ctx->ws);
-  return qr_launch(p, ctx->stream);
+  return run_qr(ctx, p);
 }
 
 }  // extern "C"

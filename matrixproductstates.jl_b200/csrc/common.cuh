@@ -99,7 +99,9 @@ struct QrProblem {
   cd* R = nullptr;       int64_t r_r = 0, r_c = 0, r_b = 0;   // optional n x n upper-triangular factor
   int* err = nullptr;    // device word; a bounded wait that runs out sets bit 0 (may be null)
 };
-int qr_launch(const QrProblem& p, cudaStream_t s);
+struct Workspace;
+// Q (and R) of each problem; uses the workspace's QR scratch (V, tau, V^H V, T V1^H)
+int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s);
 bool qr_supported(int m, int n);
 
 }  // namespace mpsb

@@ -160,6 +160,15 @@ int op_update_lenv(mpsb_ctx* ctx, const cd* A0, const cd* AL, cd* env, int lead,
   return run_gemm(ctx, g);
 }
 
+// QR through the context's workspace; a reallocated QR scratch invalidates captured graphs
+int run_qr(mpsb_ctx* ctx, const QrProblem& p) {
+  void* before = ctx->ws.qr.p;
+  count_launch(&ctx->ws);
+  int st = qr_launch(p, &ctx->ws, ctx->stream);
+  if (ctx->ws.qr.p != before) ctx->ws_generation++;
+  return st;
+}
+
 // leftorth! / leftorth (src/orthonormalisation.jl:150-171): Q of reshape(A, Dl*d, Dr), in place
 int op_orth_left(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr, cd* R) {
   QrProblem p;
@@ -168,8 +177,7 @@ int op_orth_left(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr, cd* R) {
   p.Q = A; p.q_r = 1; p.q_c = (int64_t)Dl * d;
   if (R) { p.R = R; p.r_r = 1; p.r_c = Dr; }
   p.err = ctx->err();
-  count_launch(&ctx->ws);
-  return qr_launch(p, ctx->stream);
+  return run_qr(ctx, p);
 }
 
 // rightorth! (src/orthonormalisation.jl:227-234): QR of the non-conjugate transpose
@@ -180,8 +188,7 @@ int op_orth_right(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr) {
   p.X = A; p.x_r = Dl; p.x_c = 1;
   p.Q = A; p.q_r = Dl; p.q_c = 1;
   p.err = ctx->err();
-  count_launch(&ctx->ws);
-  return qr_launch(p, ctx->stream);
+  return run_qr(ctx, p);
 }
 
 // ------------------------------------------------------------------------------------

@@ -96,6 +96,7 @@ int op_A3_R2(mpsb_ctx* ctx, const cd* A, const cd* R, cd* out, int lead, int chi
 int op_update_renv(mpsb_ctx* ctx, const cd* A0, const cd* AR, cd* env, int chiA, int chiL0, int drest);
 int op_update_lenv(mpsb_ctx* ctx, const cd* A0, const cd* AL, cd* env, int lead, int chiR0, int y, bool conj);
 // QR of a site: left (reshape(A, Dl*d, Dr)) or right (transpose of reshape(A, Dl, d*Dr))
+int run_qr(mpsb_ctx* ctx, const QrProblem& p);
 int op_orth_left(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr, cd* R /* Dr x Dr or null */);
 int op_orth_right(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr);
 

@@ -19,13 +19,18 @@
 // barrier sits inside the loops.
 //   * column j: each warp reduces its panel columns over the CTA's rows with warp shuffles
 //     (lane = row) and pushes the sums to all C CTAs; the owner of row j pushes that row;
-//     after the wait every warp recomputes the reflector, w = v^H A and the new column of
-//     the compact-WY factor T redundantly in registers, and updates its columns;
+//     after the wait warp 0 forms the reflector, w = v^H A and the new column of the
+//     compact-WY factor T, and every warp updates its columns;
 //   * trailing columns: partials of V^H A pushed to the owner of each column slice,
 //     reduced there in a fixed order with T^H applied, the slice pushed to every CTA,
-//     then A -= V W locally;
-//   * Q formation runs the panels backwards: Q_trail -= V (T (V^H Q_trail)) with the same
-//     two exchanges, the panel block built as E - V (T V1^H) from the pushed top block V1.
+//     then A -= V W locally.
+// The cluster kernel ends with R, the explicit reflectors V (m x n, unit lower trapezoidal)
+// and tau in global memory, and E = [I; 0] in Q.  Q is then formed on the whole GPU with the
+// UT-transform identity  Q = (I - V T V^H) E = E - V (T V1^H),  T^{-1} = diag(1/tau) +
+// striu(V^H V)  (V1 = top n x n block of V): a tensor-core GEMM for G = V^H V, one
+// back-substitution kernel for M = T V1^H (T^{-1} M = V1^H, so M[i,:] = tau_i (V1^H[i,:] -
+// sum_{k>i} G[i,k] M[k,:]) needs no division and gives M[i,:] = 0 when tau_i = 0), and a
+// tensor-core GEMM for Q -= V M.  In exact arithmetic this is zungqr's Q.
 // Reductions run in a fixed order, so every CTA computes bit-identical reflectors and
 // results are reproducible run to run.  Each wait gives up after a bounded number of polls,
 // records the timeout in the error word and lets the kernel run to completion.
@@ -35,6 +40,7 @@
 #include <cstdlib>
 
 #include "common.cuh"
+#include "workspace.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -45,13 +51,15 @@ constexpr int NT = 256, NW = 8;
 constexpr int CMAX = 16;
 constexpr size_t SMEM_LIMIT = 227 * 1024;
 constexpr int WAIT_LIMIT = 1 << 22;
-enum { MB_COL0 = 0, MB_COL1, MB_RS, MB_AG, MB_V10, MB_V11, MB_COUNT };
+enum { MB_COL0 = 0, MB_COL1, MB_RS, MB_AG, MB_COUNT };
 
 struct QrParams {
   QrProblem p;
+  cd* V;     // [batch][n][m] explicit unit lower trapezoidal reflectors (output)
+  cd* Tg;    // [batch][npanels][NB][NB] compact-WY factor of every panel (output)
   int C, npanels, ldS, ksmax;
   // shared-memory offsets (complex elements) and the byte offset of the mbarriers
-  int o_S, o_rcol, o_rrs, o_w2s, o_rag, o_T, o_rv1, o_mloc, o_bc, o_tst, o_mbar;
+  int o_S, o_rcol, o_rrs, o_w2s, o_rag, o_T, o_bc, o_tst, o_mbar;
 };
 
 // ---- PTX helpers -------------------------------------------------------------------
@@ -129,8 +137,7 @@ __device__ __forceinline__ cd warp_sum(cd v) {
 // rrs   [C][NB*ksmax]        partials of V^H A received from each rank for my column slice
 // w2s   [NB*ksmax]           my reduced slice
 // rag   [NB*n]               the gathered W2 (all slices)
-// T     [npanels*NB*NB]      compact-WY factors (column-major NB x NB)
-// rv1   [2][NB*NB]           pushed top block V1 of the panel (two parities);  mloc [NB*NB] = T V1^H
+// T     [NB*NB]              compact-WY factor of the current panel (column-major NB x NB)
 // mbar  [MB_COUNT] u64
 
 // V[r, i] of panel p0 for global row g (unit lower trapezoidal, stored below the diagonal)
@@ -204,8 +211,6 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
   cd* w2s = sm + P.o_w2s;
   cd* rag = sm + P.o_rag;
   cd* Tall = sm + P.o_T;
-  cd* rv1 = sm + P.o_rv1;
-  cd* mloc = sm + P.o_mloc;
   cd* bcs = sm + P.o_bc;        // tau, beta, scale of the current column
   cd* bcw = bcs + 4;            // w_c of the current column
   cd* tst = sm + P.o_tst;       // tst[jl*NB + c] = t_c (c < jl), tst[jl*NB + jl] = tau_jl
@@ -352,7 +357,7 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
       __syncthreads();
       sp ^= 1;
     }
-    cd* Tp = Tall + pi * NB * NB;
+    cd* Tp = Tall;   // the previous panel's T was last read before its all-gather wait
     // T (compact WY, zlarft forward/columnwise) from the stashed t vectors, by warp 0 while the
     // other warps start on the trailing partials: T[0:jl, jl] = -tau_jl T[0:jl, 0:jl] t_jl
     if (warp == 0) {
@@ -365,6 +370,11 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
         const cd acc = cadd(cadd(a4[0], a4[1]), cadd(a4[2], a4[3]));
         if (lane < NB) Tp[lane + NB * jl] = (lane < jl) ? cmul(cmk(-tj.x, -tj.y), acc) : (lane == jl ? tj : cmk(0.0, 0.0));
         __syncwarp();
+      }
+      if (crank == 0 && lane < NB) {   // lane-owned entries of T, zero outside the panel width
+        cd* Tout = P.Tg + ((int64_t)prob * P.npanels + pi) * NB * NB;
+        for (int jl = 0; jl < NB; ++jl)
+          Tout[lane + NB * jl] = (lane < pw && jl < pw) ? Tp[lane + NB * jl] : cmk(0.0, 0.0);
       }
     }
 
@@ -429,104 +439,14 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
       Rout[(int64_t)g * P.p.r_r + (int64_t)k * P.p.r_c] = (k >= g) ? S[k * ldS + rr] : cmk(0.0, 0.0);
     }
   }
-  // rows above each column's panel start are zero in the partially formed Q
-  for (int e = tid; e < ROWS * n; e += NT) {
-    int rr = e % ROWS, k = e / ROWS, g = row0 + rr;
-    if (g < (k / NB) * NB) S[k * ldS + rr] = cmk(0.0, 0.0);
-  }
-  __syncthreads();
-
-  // ================================ Q formation ==================================
-  int vp = 0;
-  for (int pi = P.npanels - 1; pi >= 0; --pi) {
-    const int p0 = pi * NB;
-    const int pw = min(NB, n - p0);
-    const int nt = n - p0 - pw, kb = p0 + pw;
-    const cd* Tp = Tall + pi * NB * NB;
-    const int KS = nt > 0 ? (nt + C - 1) / C : 1;
-    const int k0 = crank * KS, ks_mine = max(0, min(nt, k0 + KS) - k0);
-    cd* v1 = rv1 + vp * NB * NB;
-    const uint32_t mbv = mbs[MB_V10 + vp];
-    // partials of V^H Q_trail pushed to slice owners; top block V1 pushed to every CTA
-    if (nt > 0) partials_push<ROWS, NB>(S, ldS, rrs, mbs[MB_RS], crank, ksmax, row0, m, p0, pw, kb, nt, KS, tid, NT);
-    for (int e = tid; e < pw * pw; e += NT) {
-      const int c = e % pw, i = e / pw, g = p0 + c;
-      if (g >= row0 && g < row0 + ROWS) {
-        const cd v = (c == i) ? cmk(1.0, 0.0) : (c > i ? S[(p0 + i) * ldS + (g - row0)] : cmk(0.0, 0.0));
-        const uint32_t la = su32(&v1[c + NB * i]);
-        for (int q = 0; q < C; ++q) st_async(mapa(la, q), v, mapa(mbv, q));
-      }
-    }
-    if (nt > 0) {
-      if (tid == 0) mbar_expect(mbs[MB_RS], (uint32_t)(C * pw * ks_mine * sizeof(cd)));
-      cta_wait(mbs[MB_RS], ph[MB_RS], failed, err);
-      ph[MB_RS] ^= 1;
-      for (int e = tid; e < pw * ks_mine; e += NT) {
-        const int i = e % pw, kk = e / pw;
-        cd s = cmk(0.0, 0.0);
-        s = sum_ranks(rrs + i + NB * kk, NB * ksmax, C);
-        w2s[i + NB * kk] = s;
-      }
-    }
-    // M = T V1^H  (M[i, c] = sum_{i2 = i..c} T[i, i2] conj(V1[c, i2])), read before any AG push
-    if (tid == 0) mbar_expect(mbv, (uint32_t)(pw * pw * sizeof(cd)));
-    cta_wait(mbv, ph[MB_V10 + vp], failed, err);
-    ph[MB_V10 + vp] ^= 1;
-    for (int e = tid; e < pw * pw; e += NT) {
-      const int i = e % pw, c = e / pw;
-      cd s = cmk(0.0, 0.0);
-      for (int i2 = i; i2 <= c; ++i2) cfma(s, Tp[i + NB * i2], cconj(v1[c + NB * i2]));
-      mloc[i + NB * c] = s;
-    }
-    __syncthreads();
-    if (nt > 0) {
-      // W2 = T W on my slice, pushed to every CTA
-      for (int e = tid; e < pw * ks_mine; e += NT) {
-        const int i = e % pw, kk = e / pw;
-        cd s = cmk(0.0, 0.0);
-        for (int i2 = i; i2 < pw; ++i2) cfma(s, Tp[i + NB * i2], w2s[i2 + NB * kk]);
-        const uint32_t la = su32(&rag[i + NB * (k0 + kk)]);
-        for (int q = 0; q < C; ++q) st_async(mapa(la, q), s, mapa(mbs[MB_AG], q));
-      }
-      if (tid == 0) mbar_expect(mbs[MB_AG], (uint32_t)(pw * nt * sizeof(cd)));
-      cta_wait(mbs[MB_AG], ph[MB_AG], failed, err);
-      ph[MB_AG] ^= 1;
-    }
-    // Q_trail -= V W2 and the panel block Q[g, p0 + c] = delta(g, p0 + c) - sum_i V[g, i] M[i, c];
-    // thread = (row, column group) with its V row in registers, read before the panel is rewritten
-    {
-      constexpr int G = NT / ROWS;
-      const int rr = tid % ROWS, grp = tid / ROWS, g = row0 + rr;
-      cd v[NB];
-      load_vrow<NB>(v, S, ldS, rr, g, m, p0, pw);
-      __syncthreads();
-      if (g >= p0 && g < m) {
-        for (int k = grp; k < nt; k += G) {
-          cd acc = cmk(0.0, 0.0);
-#pragma unroll
-          for (int i = 0; i < NB; ++i)
-              if (i < pw) cfma(acc, v[i], rag[i + NB * k]);
-          cd* a = &S[(kb + k) * ldS + rr];
-          *a = csub(*a, acc);
-        }
-      }
-      for (int c = grp; c < pw; c += G) {
-        cd acc = cmk(0.0, 0.0);
-#pragma unroll
-        for (int i = 0; i < NB; ++i)
-          if (i < pw) cfma(acc, v[i], mloc[i + NB * c]);
-        S[(p0 + c) * ldS + rr] = csub((g == p0 + c) ? cmk(1.0, 0.0) : cmk(0.0, 0.0), acc);
-      }
-    }
-    __syncthreads();
-    vp ^= 1;
-  }
-
-  {  // ---- write Q (this CTA's rows)
+  {  // ---- V (unit lower trapezoidal, explicit), tau, and E = [I; 0] into Q (this CTA's rows)
+    cd* V = P.V + (int64_t)prob * m * n;
     cd* Q = P.p.Q + (int64_t)prob * P.p.q_b;
     for (int e = tid; e < ROWS * n; e += NT) {
       int rr = e % ROWS, cc = e / ROWS, g = row0 + rr;
-      if (g < m) Q[(int64_t)g * P.p.q_r + (int64_t)cc * P.p.q_c] = S[cc * ldS + rr];
+      if (g >= m) continue;
+      V[g + (int64_t)cc * m] = g < cc ? cmk(0.0, 0.0) : (g == cc ? cmk(1.0, 0.0) : S[cc * ldS + rr]);
+      Q[(int64_t)g * P.p.q_r + (int64_t)cc * P.p.q_c] = cmk(g == cc ? 1.0 : 0.0, 0.0);
     }
   }
   // no CTA leaves while a peer may still address its shared memory
@@ -564,14 +484,116 @@ size_t layout(QrParams& P, int n, int C, int rows, int nb) {
   P.o_rrs = o;   o += C * nb * P.ksmax;
   P.o_w2s = o;   o += nb * P.ksmax;
   P.o_rag = o;   o += nb * n;
-  P.o_T = o;     o += P.npanels * nb * nb;
-  P.o_rv1 = o;   o += 2 * nb * nb;
-  P.o_mloc = o;  o += nb * nb;
+  P.o_T = o;     o += nb * nb;
   P.o_bc = o;    o += 4 + nb;        // tau, beta, scale, pad; w[nb]
   P.o_tst = o;   o += nb * nb;       // t vectors (and tau) of the panel's columns
   P.o_mbar = o * (int)sizeof(cd);
   return (size_t)P.o_mbar + MB_COUNT * sizeof(uint64_t);
 }
+
+// ---- M = T V1^H by block back substitution over the panels.  T^{-1} = diag(1/tau) +
+// striu(V^H V) is block upper triangular and its diagonal blocks are the inverses of the
+// panels' compact-WY factors T_p, so with G = V^H V and B = V1^H (upper triangular):
+//   M_p = T_p (B_p - sum_{q > p} G_pq M_q),  p = last panel .. 0.
+// One warp per column c of M (M is upper triangular: rows <= c), lanes over rows
+// (r = lane + 32 q), holding y = B[:, c] minus the updates so far.  Per panel: the panel's
+// rows of y are broadcast by shuffles, M_p = T_p y_p lands in the lanes of those rows, and
+// y -= G[:, panel] M_p updates the rows above.  The needed columns of G are staged in shared
+// memory one panel ahead (cp.async, double-buffered); the panels' T_p are staged once.
+constexpr int TR_WARPS = 8;
+
+template <int QMAX>
+__global__ void __launch_bounds__(32 * TR_WARPS) qr_tmat_kernel(int m, int n, int nb, const cd* __restrict__ Vg,
+                                                                 const cd* __restrict__ Tg,
+                                                                 const cd* __restrict__ Gg, cd* __restrict__ Mg) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd* Gs = reinterpret_cast<cd*>(smem_raw);   // [2][nb][n]
+  cd* Ts = Gs + 2 * nb * n;                    // [npan][nb][nb]
+  const int prob = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int npan = (n + nb - 1) / nb;
+  const cd* V = Vg + (int64_t)prob * m * n;
+  const cd* T = Tg + (int64_t)prob * npan * nb * nb;
+  const cd* G = Gg + (int64_t)prob * n * n;
+  cd* M = Mg + (int64_t)prob * n * n;
+  const int c = blockIdx.x * TR_WARPS + warp;
+  const int ctop = min(n, (blockIdx.x + 1) * TR_WARPS) - 1;   // highest column in this CTA
+
+  cd y[QMAX];
+#pragma unroll
+  for (int q = 0; q < QMAX; ++q) {
+    const int r = lane + 32 * q;
+    y[q] = (c < n && r <= c) ? cconj(V[c + (int64_t)r * m]) : cmk(0.0, 0.0);
+  }
+  if (c < n)   // panels wholly below row c stay zero
+    for (int i = (c / nb + 1) * nb + lane; i < n; i += 32) M[i + (int64_t)c * n] = cmk(0.0, 0.0);
+
+  auto stage = [&](int pi, int buf) {   // G[r, p0 + j], r < p0, j < pw
+    const int p0 = pi * nb, pw = min(nb, n - p0);
+    cd* dst = Gs + buf * nb * n;
+    for (int e = threadIdx.x; e < pw * p0; e += blockDim.x) {
+      const int r = e % p0, jj = e / p0;
+      const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(dst + jj * n + r));
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(G + r + (int64_t)(p0 + jj) * n));
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  const int pstart = ctop / nb;
+  for (int e = threadIdx.x; e < (pstart + 1) * nb * nb; e += blockDim.x) {   // T of panels 0 .. pstart
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(Ts + e));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(T + e));
+  }
+  stage(pstart, 0);   // the same commit group as T
+  for (int pi = pstart; pi >= 0; --pi) {
+    const int k = pstart - pi;
+    if (pi > 0) {
+      stage(pi - 1, (k + 1) & 1);
+      asm volatile("cp.async.wait_group 1;\n" ::);
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::);
+    }
+    __syncthreads();
+    const int p0 = pi * nb, pw = min(nb, n - p0);
+    if (c < n && p0 <= c) {   // warp-uniform
+      const int qb = p0 >> 5, base = p0 & 31, ii = lane - base;   // the panel's rows sit in lanes base ..
+      cd yb = cmk(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < QMAX; ++q)
+        if (q == qb) yb = y[q];
+      const cd* Tp = Ts + pi * nb * nb;
+      cd a0 = cmk(0.0, 0.0), a1 = cmk(0.0, 0.0);
+      for (int jj = 0; jj < pw; ++jj) {
+        const cd rj = cmk(__shfl_sync(0xffffffffu, yb.x, base + jj), __shfl_sync(0xffffffffu, yb.y, base + jj));
+        if (ii >= 0 && ii <= jj) cfma((jj & 1) ? a1 : a0, Tp[ii + nb * jj], rj);
+      }
+      const cd mi = cadd(a0, a1);
+      if (ii >= 0 && ii < pw) M[p0 + ii + (int64_t)c * n] = mi;
+      const cd* Gc = Gs + (k & 1) * nb * n;
+      for (int jj = 0; jj < pw; ++jj) {
+        const cd mj = cmk(__shfl_sync(0xffffffffu, mi.x, base + jj), __shfl_sync(0xffffffffu, mi.y, base + jj));
+        const cd* gcol = Gc + jj * n;
+#pragma unroll
+        for (int q = 0; q < QMAX; ++q) {
+          const int r = lane + 32 * q;
+          if (r < p0) y[q] = csub(y[q], cmul(gcol[r], mj));
+        }
+      }
+    }
+    __syncthreads();   // this buffer is refilled by the next iteration's prefetch
+  }
+}
+
+typedef void (*TmatKernel)(int, int, int, const cd*, const cd*, const cd*, cd*);
+
+TmatKernel tmat_kernel_for(int n) {
+  if (n <= 32) return qr_tmat_kernel<1>;
+  if (n <= 64) return qr_tmat_kernel<2>;
+  if (n <= 128) return qr_tmat_kernel<4>;
+  if (n <= 256) return qr_tmat_kernel<8>;
+  if (n <= 512) return qr_tmat_kernel<16>;
+  return nullptr;
+}
+
+size_t tmat_smem(int n, int nb) { return (2 * (size_t)nb * n + (size_t)((n + nb - 1) / nb) * nb * nb) * sizeof(cd); }
 
 struct Choice {
   int C = 0, rpl = 0, nb = 0;
@@ -594,7 +616,7 @@ bool choose(int m, int n, Choice& ch) {
     if (C > CMAX) continue;
     for (int nb : {16, 8, 4}) {
       size_t b = layout(P, n, C, rows, nb);
-      if (b <= SMEM_LIMIT) {
+      if (b <= SMEM_LIMIT && tmat_smem(n, nb) <= SMEM_LIMIT && n <= 512) {
         ch.C = C; ch.rpl = rpl; ch.nb = nb; ch.smem = b;
         return true;
       }
@@ -610,17 +632,31 @@ bool qr_supported(int m, int n) {
   return m >= n && n >= 1 && choose(m, n, ch);
 }
 
-int qr_launch(const QrProblem& p, cudaStream_t s) {
+int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s) {
   if (p.m < p.n || p.n < 1 || p.batch < 1) return MPSB_ERR_DIMENSION;
   if (p.batch > 65535) return MPSB_ERR_UNSUPPORTED;
+  if (!ws) return MPSB_ERR_INVALID_ARG;
   Choice ch;
-  if (!choose(p.m, p.n, ch)) {
+  const TmatKernel tk = tmat_kernel_for(p.n);
+  if (!choose(p.m, p.n, ch) || !tk) {
     set_last_message("QR of a %d x %d matrix exceeds the cluster shared-memory capacity", p.m, p.n);
     return MPSB_ERR_UNSUPPORTED;
   }
+  const int m = p.m, n = p.n, nb = ch.nb, npan = (n + nb - 1) / nb;
+  // scratch: V [batch][n][m], the panels' T [batch][npan][nb][nb], G = V^H V and
+  // M = T V1^H [batch][n][n] each
+  const size_t nV = (size_t)p.batch * m * n, nT = (size_t)p.batch * npan * nb * nb, nG = (size_t)p.batch * n * n;
+  MPSB_TRY(devbuf_ensure(ws, ws->qr, (nV + nT + 2 * nG) * sizeof(cd)));
+  cd* Vb = static_cast<cd*>(ws->qr.p);
+  cd* Tb = Vb + nV;
+  cd* Gb = Tb + nT;
+  cd* Mb = Gb + nG;
+
   QrParams P;
-  layout(P, p.n, ch.C, 32 * ch.rpl, ch.nb);
+  layout(P, n, ch.C, 32 * ch.rpl, ch.nb);
   P.p = p;
+  P.V = Vb;
+  P.Tg = Tb;
   QrKernel fn = kernel_for(ch.rpl, ch.nb);
   if (!fn) return MPSB_ERR_UNSUPPORTED;
   static bool attr_done[3][8] = {};
@@ -643,6 +679,38 @@ int qr_launch(const QrProblem& p, cudaStream_t s) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   MPSB_CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, P));
+
+  const cd one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0), mone = cmk(-1.0, 0.0);
+  {  // G = V^H V
+    Gemm g;
+    g.M = n; g.N = n; g.K = m; g.batch = p.batch;
+    g.A = Vb; g.a_m = m; g.a_k = 1; g.a_b = (int64_t)m * n; g.conjA = true;
+    g.B = Vb; g.b_k = 1; g.b_n = m; g.b_b = (int64_t)m * n;
+    g.C = Gb; g.c_m = 1; g.c_n = n; g.c_b = (int64_t)n * n;
+    g.alpha = one; g.beta = zero;
+    MPSB_TRY(gemm_launch(g, ws, s));
+  }
+  {  // M = T V1^H
+    const size_t smem = tmat_smem(n, nb);
+    static bool tattr[5] = {};
+    const int ti = n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : n <= 256 ? 3 : 4;
+    if (!tattr[ti]) {
+      MPSB_CUDA_TRY(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT));
+      tattr[ti] = true;
+    }
+    count_launch(ws);
+    tk<<<dim3((n + TR_WARPS - 1) / TR_WARPS, p.batch), 32 * TR_WARPS, smem, s>>>(m, n, nb, Vb, Tb, Gb, Mb);
+    MPSB_CUDA_TRY(cudaGetLastError());
+  }
+  {  // Q = E - V M  (Q holds E)
+    Gemm g;
+    g.M = m; g.N = n; g.K = n; g.batch = p.batch;
+    g.A = Vb; g.a_m = 1; g.a_k = m; g.a_b = (int64_t)m * n;
+    g.B = Mb; g.b_k = 1; g.b_n = n; g.b_b = (int64_t)n * n;
+    g.C = p.Q; g.c_m = p.q_r; g.c_n = p.q_c; g.c_b = p.q_b;
+    g.alpha = mone; g.beta = one;
+    MPSB_TRY(gemm_launch(g, ws, s));
+  }
   return MPSB_OK;
 }
 
