@@ -293,7 +293,11 @@ def run_ours(args, rank, world, local_rank, dist):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
+        # one NVTX range per timed step, so a profiler can keep exactly these launches
+        # (ncu --nvtx --nvtx-include "rk4_step/")
+        torch.cuda.nvtx.range_push("rk4_step")
         b.step()
+        torch.cuda.nvtx.range_pop()
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
