@@ -31,9 +31,11 @@ for _p in (ROOT, PKG):
 WORKLOAD = dict(na=40, d=4, chi=128, w=8, dt=0.005, gam_eg=0.1, omega=0.5, gam_phi=0.1)
 METRIC = "MPS site-updates/s (RK4 step, complex128)"
 UNIT = "site-updates/s"
-# dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel at this workload,
-# from one ncu capture (profiles/zgemm_rho40.md); None until captured
-TRAFFIC_BYTES = None
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch, from one ncu capture each:
+# qr_kernel at the workload's interior-site QR shape (512 x 128; the input read once, the
+# outputs stay in L2) and zgemm_kernel at the 3-index prod_LR shape (M=128, N=512, K=1024)
+QR_TRAFFIC_BYTES = 1114624
+GEMM_TRAFFIC_BYTES = 10551296
 
 
 def dims_rule(na, dmax, d):
@@ -263,6 +265,32 @@ def time_gemm_mix(K, ctx, torch, stream):
     return flops, secs, len(calls)
 
 
+def time_qr(ctx, torch, stream):
+    """CUDA-event timing of one QR of the interior-site shape (d*chi x chi) through the op API:
+    returns (algorithmic flops, seconds) per QR."""
+    import ctypes as C
+    from mpsb200 import _lib
+    W = WORKLOAD
+    m, n = W["d"] * W["chi"], W["chi"]
+    g = torch.Generator(device="cuda").manual_seed(7)
+    X = torch.randn(m * n, dtype=torch.complex128, device="cuda", generator=g)
+    Q = torch.empty_like(X)
+    torch.cuda.synchronize()
+    args = (C.c_void_p(X.data_ptr()), C.c_void_p(Q.data_ptr()), None, m, n)
+    for _ in range(3):
+        _lib.call("mpsb_op_qr", ctx.h, *args)
+    ctx.sync()
+    reps = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        _lib.call("mpsb_op_qr", ctx.h, *args)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    return 16.0 * (m * n * n - n ** 3 / 3.0), e0.elapsed_time(e1) / 1e3 / reps, m, n
+
+
 def run_ours(args, rank, world, local_rank, dist):
     import numpy as np
     import torch
@@ -346,16 +374,26 @@ def run_ours(args, rank, world, local_rank, dist):
         e2e_secs = float(t.item())
     e2e_value = world * W["na"] * ke / e2e_secs
 
-    # ---- roofline of the dominant kernel (zgemm) on this workload's GEMM shapes
-    gflops, gsecs, ncalls = time_gemm_mix(K, ctx, torch, stream)
+    # ---- roofline of the dominant kernel (the cluster QR, ~43% of the step by the ncu launch
+    # list) at the workload's interior-site shape, and of the zgemm kernel on the site's GEMMs
     peak = measure_fp64_peak(torch)
-    achieved = gflops / gsecs / 1e12
-    roofline = {"bound": "tensor", "pipe": "fp64", "kernel": "zgemm_kernel",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+    qflops, qsecs, qm, qn = time_qr(ctx, torch, stream)
+    qach = qflops / qsecs / 1e12
+    roofline = {"bound": "tensor", "pipe": "fp64", "limiter": "latency (128 sequential column steps)",
+                "kernel": "qr_kernel (cluster Householder factorisation) + Q formation (2 zgemm_kernel, qr_tmat_kernel)",
+                "achieved": qach, "peak": peak, "unit": "TFLOP/s", "frac": qach / peak,
                 "peak_source": "cuBLAS zgemm 4096^3 measured in this run (no FP64 entry in MEASURED_PEAKS.json)",
-                "traffic": TRAFFIC_BYTES,
-                "per_launch": "flop-weighted mean over the %d GEMM shapes of an interior site "
-                              "(chi=128, d=4, w=8): %.3e flops in %.1f us" % (ncalls, gflops, gsecs * 1e6)}
+                "traffic": QR_TRAFFIC_BYTES,
+                "per_launch": "one QR of %d x %d (d*chi x chi): 16(mn^2 - n^3/3) = %.3e flops in %.1f us; "
+                              "traffic = qr_kernel dram read+write (ncu)" % (qm, qn, qflops, qsecs * 1e6)}
+    gflops, gsecs, ncalls = time_gemm_mix(K, ctx, torch, stream)
+    gach = gflops / gsecs / 1e12
+    roofline_gemm = {"bound": "tensor", "pipe": "fp64", "kernel": "zgemm_kernel",
+                     "achieved": gach, "peak": peak, "unit": "TFLOP/s", "frac": gach / peak,
+                     "traffic": GEMM_TRAFFIC_BYTES,
+                     "per_launch": "flop-weighted mean over the %d GEMM shapes of an interior site "
+                                   "(chi=128, d=4, w=8): %.3e flops in %.1f us; traffic = the prod_LR launch "
+                                   "(M=128, N=512, K=1024) dram read+write (ncu)" % (ncalls, gflops, gsecs * 1e6)}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
@@ -367,6 +405,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "step_tflops": sum(fl.values()) * args.steps / secs * world / 1e12,
         "step_flops": fl,
         "roofline": roofline,
+        "roofline_gemm": roofline_gemm,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16,
                 "steps": ke},
         "check": {"trace_rho": tr.real, "max_see": float(np.max(see.real))},
