@@ -118,6 +118,21 @@ int mpsb_compress_sum_var_apply_H_left(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* co
 int mpsb_compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain,
                               const mpsb_mps* A, const mpsb_mpo* H, int maxsweeps);
 
+/* compress_sum_var_apply_H!(A0, envop, coef, A, H, maxsweeps)  src/compression.jl:805-887
+ * maxsweeps R->L / L->R sweep pairs compressing sum_{l<numv-1} coef[l] A[l] + coef[numv-1] H A[numv-1]
+ * into A0, which is both the initial guess and the output (it must not be one of the terms).
+ * coef is numv interleaved complex; numv in 2..9.  The plain-term environments are internal. */
+int mpsb_compress_sum_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const double* coef,
+                                  int numv, mpsb_mps* const* A, const mpsb_mpo* H, int maxsweeps);
+
+/* compress_sum_var(Ain, coef, A, maxsweeps)  src/compression.jl:496-565
+ * The same without an operator (every term plain, numv in 1..8): A0 = the compression of
+ * sum_l coef[l] A[l] with Ain as the initial guess (copied into A0 first unless A0 == Ain;
+ * A0 must not be one of the terms).  The reference returns a new MPS; here the caller
+ * passes the output handle. */
+int mpsb_compress_sum_var(mpsb_ctx* ctx, mpsb_mps* A0, const mpsb_mps* Ain, const double* coef,
+                          int numv, mpsb_mps* const* A, int maxsweeps);
+
 /* ---------------------------------------------------------------- gauge / norms
  * normalize_lo!(mps) src/orthonormalisation.jl:97-103 -> *no = sum(abs2, mps[end])
  * norm_lo(mps)       src/orthonormalisation.jl:117-121

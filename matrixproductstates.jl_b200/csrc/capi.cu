@@ -383,6 +383,33 @@ int mpsb_compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, cons
   return compress_var_apply_H(ctx, A0, envop, Ain, A, H, maxsweeps);
 }
 
+static int full_sum_var(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const double* coef, int numv,
+                        mpsb_mps* const* A, const mpsb_mpo* H, int maxsweeps) {
+  if (!coef || !A || numv < 1 || numv > 9) return MPSB_ERR_INVALID_ARG;
+  std::vector<cd> c(numv);
+  std::vector<const mpsb_mps*> t(numv);
+  for (int i = 0; i < numv; ++i) {
+    c[i] = cmk(coef[2 * i], coef[2 * i + 1]);
+    t[i] = A[i];
+  }
+  return compress_sum_var_full(ctx, A0, envop, c.data(), numv, t.data(), H, maxsweeps);
+}
+
+int mpsb_compress_sum_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const double* coef, int numv,
+                                  mpsb_mps* const* A, const mpsb_mpo* H, int maxsweeps) {
+  MPSB_TRY(bind(ctx));
+  if (!H) return MPSB_ERR_INVALID_ARG;
+  return full_sum_var(ctx, A0, envop, coef, numv, A, H, maxsweeps);
+}
+
+int mpsb_compress_sum_var(mpsb_ctx* ctx, mpsb_mps* A0, const mpsb_mps* Ain, const double* coef, int numv,
+                          mpsb_mps* const* A, int maxsweeps) {
+  MPSB_TRY(bind(ctx));
+  if (!A0 || !Ain) return MPSB_ERR_INVALID_ARG;
+  if (A0 != Ain) MPSB_TRY(mpsb_mps_copy(A0, Ain));   // the guess
+  return full_sum_var(ctx, A0, nullptr, coef, numv, A, nullptr, maxsweeps);
+}
+
 // ---------------------------------------------------------------- gauge / norms
 int mpsb_norm_lo(mpsb_ctx* ctx, const mpsb_mps* A, double* no) {
   MPSB_TRY(bind(ctx));

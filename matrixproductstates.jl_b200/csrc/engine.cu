@@ -210,12 +210,17 @@ static int sweep_scratch(mpsb_ctx* ctx, const mpsb_mps* A0, const mpsb_mpo* H, i
   const int d = A0->d;
   for (int k = 0; k < A0->na; ++k) {
     int64_t Dl = A0->dims[k], Dr = A0->dims[k + 1];
-    maxAOR = std::max<int64_t>(maxAOR, Dl * H->w[k] * d * Dr);
-    maxAOL = std::max<int64_t>(maxAOL, Dl * d * Dr * H->w[k + 1]);
+    if (H) {
+      maxAOR = std::max<int64_t>(maxAOR, Dl * H->w[k] * d * Dr);
+      maxAOL = std::max<int64_t>(maxAOL, Dl * d * Dr * H->w[k + 1]);
+    }
     maxSite = std::max<int64_t>(maxSite, Dl * d * Dr);
   }
-  MPSB_TRY(ensure_slot(ctx, SLOT_AOR, maxAOR * sizeof(cd), &s.AOR));
-  MPSB_TRY(ensure_slot(ctx, SLOT_AOL, maxAOL * sizeof(cd), &s.AOL));
+  s.AOR = s.AOL = nullptr;
+  if (H) {
+    MPSB_TRY(ensure_slot(ctx, SLOT_AOR, maxAOR * sizeof(cd), &s.AOR));
+    MPSB_TRY(ensure_slot(ctx, SLOT_AOL, maxAOL * sizeof(cd), &s.AOL));
+  }
   if (nplain > 8) return MPSB_ERR_UNSUPPORTED;
   cd* base = nullptr;
   if (nplain > 0) MPSB_TRY(ensure_slot(ctx, SLOT_P0, (size_t)nplain * maxSite * sizeof(cd), &base));
@@ -356,6 +361,110 @@ int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mps
     }
   }
   return MPSB_OK;
+}
+
+// compress_sum_var_apply_H! (src/compression.jl:805-887) when H is given -- the last term is
+// H * A[numv-1] with its coefficient at envop's right boundary -- and compress_sum_var
+// (src/compression.jl:496-565) when H is null (every term plain): maxsweeps R->L / L->R sweep
+// pairs of the variational compression of the weighted sum, then the last site.  A0 is the
+// guess (the bra of the initial left environments) and is overwritten with the result; it
+// must not be one of the terms.  The plain-term environments live in context scratch.
+int compress_sum_var_full(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const cd* coef, int numv,
+                          const mpsb_mps* const* A, const mpsb_mpo* H, int maxsweeps) {
+  if (!ctx || !A0 || !coef || !A || numv < 1 || maxsweeps < 0) return MPSB_ERR_INVALID_ARG;
+  const bool hasH = H != nullptr;
+  if (hasH && !envop) return MPSB_ERR_INVALID_ARG;
+  const int np = hasH ? numv - 1 : numv;
+  if (np < 1) {   // the reference indexes the first plain term unconditionally
+    set_last_message("compress_sum_var: at least one plain term is required");
+    return MPSB_ERR_INVALID_ARG;
+  }
+  if (np > 8) return MPSB_ERR_UNSUPPORTED;
+  for (int l = 0; l < numv; ++l) {
+    if (!A[l] || !same_dims(A0, A[l])) return MPSB_ERR_DIMENSION;
+    if (A[l] == A0 || A[l]->slab == A0->slab) {
+      set_last_message("compress_sum_var: the output MPS must not be one of the terms");
+      return MPSB_ERR_INVALID_ARG;
+    }
+  }
+  const int na = A0->na, d = A0->d;
+  if (hasH) {
+    if (!envop->three || envop->na != na || H->na != na || H->d != d) return MPSB_ERR_DIMENSION;
+    for (int k = 0; k <= na; ++k)
+      if (envop->d1[k] != A0->dims[k] || envop->d2[k] != A0->dims[k] || envop->w[k] != H->w[k])
+        return MPSB_ERR_DIMENSION;
+  }
+  SweepScratch s;
+  MPSB_TRY(sweep_scratch(ctx, A0, H, np, s));
+  auto D = [&](int k) { return (int)A0->dims[k]; };
+  auto W = [&](int k) { return (int)H->w[k]; };
+  std::vector<int64_t> eoff(na + 1);
+  int64_t etot = 0;
+  for (int k = 0; k <= na; ++k) {
+    eoff[k] = etot;
+    etot += A0->dims[k] * A0->dims[k];
+  }
+  cd* ebase = nullptr;
+  MPSB_TRY(ensure_slot(ctx, SLOT_SUMENV, (size_t)np * etot * sizeof(cd), &ebase));
+  auto E = [&](int l, int k) { return ebase + (int64_t)l * etot + eoff[k]; };
+  const mpsb_mps* AH = hasH ? A[np] : nullptr;
+
+  // ---- left environments with A0 as the bra
+  for (int l = 0; l < np; ++l) {
+    MPSB_TRY(set_boundary(ctx, E(l, 0), ONE));
+    for (int k = 0; k < na - 1; ++k) {
+      MPSB_TRY(op_L2_A3(ctx, E(l, k), A[l]->site(k), s.P[l], D(k), D(k), d * D(k + 1), ONE, ZERO, false));
+      MPSB_TRY(op_update_lenv(ctx, A0->site(k), s.P[l], E(l, k + 1), D(k) * d, D(k + 1), D(k + 1), true));
+    }
+    MPSB_TRY(set_boundary(ctx, E(l, na), coef[l]));
+  }
+  if (hasH) {
+    MPSB_TRY(set_boundary(ctx, envop->entry(0), ONE));
+    for (int k = 0; k < na - 1; ++k) {
+      MPSB_TRY(op_prod_AOL(ctx, AH->site(k), H->site(k), envop->entry(k), s.AOL, D(k), d, D(k + 1), W(k), W(k + 1), D(k)));
+      MPSB_TRY(op_update_le(ctx, A0->site(k), s.AOL, envop->entry(k + 1), D(k), d, D(k + 1), W(k + 1), D(k + 1)));
+    }
+    MPSB_TRY(set_boundary(ctx, envop->entry(na), coef[np]));
+  }
+  // site k of the L->R direction: plain terms, then the H term, accumulated into A0[k]
+  auto site_lr = [&](int k) -> int {
+    cd* out = A0->site(k);
+    for (int l = 0; l < np; ++l) {
+      MPSB_TRY(op_L2_A3(ctx, E(l, k), A[l]->site(k), s.P[l], D(k), D(k), d * D(k + 1), ONE, ZERO, false));
+      MPSB_TRY(op_A3_R2(ctx, s.P[l], E(l, k + 1), out, D(k) * d, D(k + 1), D(k + 1), ONE, l ? ONE : ZERO));
+    }
+    if (hasH) {
+      MPSB_TRY(op_prod_AOL(ctx, AH->site(k), H->site(k), envop->entry(k), s.AOL, D(k), d, D(k + 1), W(k), W(k + 1), D(k)));
+      MPSB_TRY(op_prod_LR_4_3(ctx, s.AOL, envop->entry(k + 1), out, D(k), d, D(k + 1), W(k + 1), D(k + 1), ONE, ONE));
+    }
+    return MPSB_OK;
+  };
+  for (int sw = 0; sw < maxsweeps; ++sw) {
+    for (int k = na - 1; k >= 1; --k) {   // sweep left
+      cd* out = A0->site(k);
+      for (int l = 0; l < np; ++l) {
+        MPSB_TRY(op_A3_R2(ctx, A[l]->site(k), E(l, k + 1), s.P[l], D(k) * d, D(k + 1), D(k + 1), ONE, ZERO));
+        MPSB_TRY(op_L2_A3(ctx, E(l, k), s.P[l], out, D(k), D(k), d * D(k + 1), ONE, l ? ONE : ZERO, false));
+      }
+      if (hasH) {
+        MPSB_TRY(op_prod_AOR(ctx, AH->site(k), H->site(k), envop->entry(k + 1), s.AOR, D(k), d, D(k + 1), W(k), W(k + 1), D(k + 1)));
+        MPSB_TRY(op_prod_LR_3_4(ctx, envop->entry(k), s.AOR, out, D(k), W(k), D(k), d, D(k + 1), ONE, ONE));
+      }
+      MPSB_TRY(op_orth_right(ctx, out, D(k), d, D(k + 1)));
+      for (int l = 0; l < np; ++l)
+        MPSB_TRY(op_update_renv(ctx, out, s.P[l], E(l, k), D(k), D(k), d * D(k + 1)));
+      if (hasH) MPSB_TRY(op_update_re(ctx, out, s.AOR, envop->entry(k), D(k), W(k), d, D(k + 1), D(k)));
+    }
+    for (int k = 0; k < na - 1; ++k) {   // sweep right
+      MPSB_TRY(site_lr(k));
+      cd* out = A0->site(k);
+      MPSB_TRY(op_orth_left(ctx, out, D(k), d, D(k + 1), nullptr));
+      for (int l = 0; l < np; ++l)
+        MPSB_TRY(op_update_lenv(ctx, out, s.P[l], E(l, k + 1), D(k) * d, D(k + 1), D(k + 1), true));
+      if (hasH) MPSB_TRY(op_update_le(ctx, out, s.AOL, envop->entry(k + 1), D(k), d, D(k + 1), W(k + 1), D(k + 1)));
+    }
+  }
+  return site_lr(na - 1);
 }
 
 // RK4stp_apply_H_half! (src/timeevolution.jl:178-196)

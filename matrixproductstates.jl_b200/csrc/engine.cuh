@@ -71,7 +71,7 @@ namespace mpsb {
 // named scratch slots in Workspace::named
 enum Slot {
   SLOT_T = 0, SLOT_AOR, SLOT_G1, SLOT_AOL, SLOT_P0, SLOT_P1, SLOT_P2, SLOT_ENV0, SLOT_ENV1,
-  SLOT_MISC, SLOT_COUNT
+  SLOT_MISC, SLOT_SUMENV, SLOT_COUNT
 };
 
 int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out);
@@ -106,6 +106,8 @@ int compress_var_apply_H_left(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, cons
 int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* const* env, mpsb_env* envop,
                              const mpsb_mps* Ain, const cd* coef, int numv, const mpsb_mps* const* A,
                              const mpsb_mpo* H);
+int compress_sum_var_full(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const cd* coef, int numv,
+                          const mpsb_mps* const* A, const mpsb_mpo* H /* null: compress_sum_var */, int maxsweeps);
 int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain, const mpsb_mps* A,
                          const mpsb_mpo* H, int maxsweeps);
 int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,

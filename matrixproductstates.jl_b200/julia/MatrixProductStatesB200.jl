@@ -127,6 +127,26 @@ compress_var_apply_H!(ctx::Ctx, A0::DMPS, envop::DEnv, Ain::DMPS, A::DMPS, H::DM
                 (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Cint),
                 ctx.h, A0.h, envop.h, Ain.h, A.h, H.h, maxsweeps), :mpsb_compress_var_apply_H)
 
+# compress_sum_var_apply_H!(A0, envop, coef, A, H, maxsweeps)   src/compression.jl:805-887
+function compress_sum_var_apply_H!(ctx::Ctx, A0::DMPS, envop::DEnv, coef::Vector{<:Number}, A::Vector{DMPS},
+                                   H::DMPO, maxsweeps::Integer)
+    c = ComplexF64.(coef)
+    hs = [a.h for a in A]
+    GC.@preserve c hs check(ccall((:mpsb_compress_sum_var_apply_H, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{ComplexF64}, Cint, Ptr{Ptr{Cvoid}}, Ptr{Cvoid}, Cint),
+        ctx.h, A0.h, envop.h, c, length(c), hs, H.h, maxsweeps), :mpsb_compress_sum_var_apply_H)
+end
+
+# compress_sum_var(Ain, coef, A, maxsweeps)   src/compression.jl:496-565 (A0 = the new MPS)
+function compress_sum_var!(ctx::Ctx, A0::DMPS, Ain::DMPS, coef::Vector{<:Number}, A::Vector{DMPS},
+                           maxsweeps::Integer)
+    c = ComplexF64.(coef)
+    hs = [a.h for a in A]
+    GC.@preserve c hs check(ccall((:mpsb_compress_sum_var, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{ComplexF64}, Cint, Ptr{Ptr{Cvoid}}, Cint),
+        ctx.h, A0.h, Ain.h, c, length(c), hs, maxsweeps), :mpsb_compress_sum_var)
+end
+
 # normalize_lo!(mps)   src/orthonormalisation.jl:97-103
 function normalize_lo!(ctx::Ctx, A::DMPS)
     no = Ref{Cdouble}(0)

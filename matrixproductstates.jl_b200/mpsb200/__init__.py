@@ -5,8 +5,9 @@ include/mpsb.h).  This package is the host-side mirror of the reference API.
 """
 from ._lib import DimensionMismatch, MpsbError, load  # noqa: F401
 from .core import (  # noqa: F401
-    MPO, MPS, Context, Env, RK4stp_apply_H_half_, apply_site_operator_, applyMPOtoMPS, build_env,
-    compress_sum_var_apply_H_left_, compress_sum_var_apply_H_right_, compress_var_apply_H_,
+    MPO, MPS, Arnoldi_expm_, Context, Env, RK4stp_apply_H_half_, apply_site_operator_, applyMPOtoMPS,
+    build_env, compress_sum_var, compress_sum_var_apply_H_, compress_sum_var_apply_H_left_,
+    compress_sum_var_apply_H_right_, compress_var_apply_H_,
     compress_var_apply_H_left_, default_context, expandmps, leftorth_sites_, leftorthogonalizeQR_,
     leftorthonormalizationQR_, makemps, makempo, measure_local, mpsgroundstate, mpsproductstate,
     mpsrandom, norm_lo, normalize_lo_, scal_op_prod, scal_prod, scal_prod_no_conj,

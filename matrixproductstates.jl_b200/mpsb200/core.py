@@ -387,6 +387,54 @@ def compress_var_apply_H_(A0, envop, Ain, A, H, maxsweeps):
     _lib.call("mpsb_compress_var_apply_H", A0.ctx.h, A0.h, envop.h, Ain.h, A.h, H.h, int(maxsweeps))
 
 
+def _terms(name, coef, A):
+    numv = len(coef)
+    if len(A) != numv:
+        raise _lib.DimensionMismatch(-2, name, "len(A) must be len(coef)")
+    return numv, _coef_buf(coef), (C.c_void_p * numv)(*[a.h.value for a in A])
+
+
+def compress_sum_var_apply_H_(A0, envop, coef, A, H, maxsweeps):
+    """src/compression.jl:805-887: A0 (guess and output) <- the variational compression of
+    sum_l coef[l] A[l] + coef[-1] H A[-1] with maxsweeps sweep pairs."""
+    numv, cb, terms = _terms("compress_sum_var_apply_H!", coef, A)
+    _lib.call("mpsb_compress_sum_var_apply_H", A0.ctx.h, A0.h, envop.h, _dptr(cb), numv, terms, H.h, int(maxsweeps))
+
+
+def compress_sum_var(Ain, coef, A, maxsweeps):
+    """src/compression.jl:496-565: a new MPS compressing sum_l coef[l] A[l], guess Ain."""
+    numv, cb, terms = _terms("compress_sum_var", coef, A)
+    A0 = MPS(Ain.dims, Ain.d, Ain.ctx)
+    _lib.call("mpsb_compress_sum_var", A0.ctx.h, A0.h, Ain.h, _dptr(cb), numv, terms, int(maxsweeps))
+    return A0
+
+
+def Arnoldi_expm_(A, rhov, numv, env, envop):
+    """src/timeevolution.jl:88-119: Krylov step rhov[0] <- exp(A) rhov[0] (normalised) in the
+    span of numv MPSs built by repeated application of the MPO A (one sweep pair each, then
+    normalize_lo!), with the projected generator H and overlap matrix N measured by
+    scal_op_prod / scal_prod and coef = expm(N \\ H)[:, 0].  `env` is unused, as in the
+    reference (the plain-term environments are internal).  rhov[0] is rebound to a new MPS."""
+    import scipy.linalg
+    Nm = np.eye(numv, dtype=CT)
+    Hm = np.zeros((numv, numv), dtype=CT)
+    Hm[0, 0] = scal_op_prod(rhov[0], A, rhov[0])
+    for jj in range(1, numv):
+        coef = [-Hm[ll, jj - 1] for ll in range(jj)] + [1.0]
+        compress_sum_var_apply_H_(rhov[jj], envop, coef, list(rhov[:jj]) + [rhov[jj - 1]], A, 1)
+        normalize_lo_(rhov[jj])
+        Hm[jj, jj] = scal_op_prod(rhov[jj], A, rhov[jj])
+        for ll in range(jj):
+            Hm[jj, ll] = scal_op_prod(rhov[jj], A, rhov[ll])
+            Hm[ll, jj] = scal_op_prod(rhov[ll], A, rhov[jj])
+            Nm[jj, ll] = scal_prod(rhov[jj], rhov[ll])
+            Nm[ll, jj] = np.conj(Nm[jj, ll])
+    coef = scipy.linalg.expm(np.linalg.solve(Nm, Hm))[:, 0]
+    rhov[0] = compress_sum_var(rhov[0], list(coef), rhov, 1)
+    normalize_lo_(rhov[0])
+    return coef
+
+
 # ------------------------------------------------------------------ norms, gauge, observables
 
 def _scalar(name, *args):

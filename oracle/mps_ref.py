@@ -576,6 +576,74 @@ def compress_sum_var_apply_H_(A0, envop, coef, A, H, maxsweeps):
     A0[na - 1] = acc + prod_LR(AOL, envop[na])
 
 
+def compress_sum_var(Ain, coef, A, maxsweeps):
+    """src/compression.jl:496-565: returns the compression of sum_l coef[l] A[l], guess Ain."""
+    na = len(Ain)
+    numv = len(coef)
+    FL, FR = [], []
+    for ll in range(numv):
+        fl = [None] * na
+        fl[0] = np.ones((1, 1), dtype=CT)
+        for jj in range(na - 1):
+            fl[jj + 1] = update_lenv_full(Ain[jj], A[ll][jj], fl[jj])
+        fr = [None] * na
+        fr[na - 1] = np.full((1, 1), coef[ll], dtype=CT)
+        FL.append(fl)
+        FR.append(fr)
+    A0 = [None] * na
+    AR = [None] * numv
+    for _ in range(maxsweeps):
+        for jj in range(na - 1, 0, -1):
+            AR[0] = prod_LR(A[0][jj], FR[0][jj])
+            acc = prod_LR(FL[0][jj], AR[0])
+            for ll in range(1, numv):
+                AR[ll] = prod_LR(A[ll][jj], FR[ll][jj])
+                acc = acc + prod_LR(FL[ll][jj], AR[ll])
+            A0[jj] = rightorth_(acc)
+            for ll in range(numv):
+                FR[ll][jj - 1] = update_renv(A0[jj], AR[ll])
+        for jj in range(na - 1):
+            AR[0] = prod_LR(FL[0][jj], A[0][jj])
+            acc = prod_LR(AR[0], FR[0][jj])
+            for ll in range(1, numv):
+                AR[ll] = prod_LR(FL[ll][jj], A[ll][jj])
+                acc = acc + prod_LR(AR[ll], FR[ll][jj])
+            A0[jj] = leftorth_(acc)
+            for ll in range(numv):
+                FL[ll][jj + 1] = update_lenv(A0[jj], AR[ll])
+    AR[0] = prod_LR(FL[0][na - 1], A[0][na - 1])
+    acc = prod_LR(AR[0], FR[0][na - 1])
+    for ll in range(1, numv):
+        AR[ll] = prod_LR(FL[ll][na - 1], A[ll][na - 1])
+        acc = acc + prod_LR(AR[ll], FR[ll][na - 1])
+    A0[na - 1] = acc
+    return A0
+
+
+def Arnoldi_expm_(A, rhov, numv, env, envop):
+    """src/timeevolution.jl:88-119 (rhov[0] <- normalised Krylov approximation of exp(A) rhov[0]).
+
+    Returns coef = expm(N \\ H)[:, 0]; `env` is unused, as in the reference."""
+    import scipy.linalg
+    Nm = np.eye(numv, dtype=CT)
+    Hm = np.zeros((numv, numv), dtype=CT)
+    Hm[0, 0] = scal_op_prod(rhov[0], A, rhov[0])
+    for jj in range(1, numv):
+        coef = [-Hm[ll, jj - 1] for ll in range(jj)] + [1.0]
+        compress_sum_var_apply_H_(rhov[jj], envop, coef, list(rhov[:jj]) + [rhov[jj - 1]], A, 1)
+        normalize_lo_(rhov[jj])
+        Hm[jj, jj] = scal_op_prod(rhov[jj], A, rhov[jj])
+        for ll in range(jj):
+            Hm[jj, ll] = scal_op_prod(rhov[jj], A, rhov[ll])
+            Hm[ll, jj] = scal_op_prod(rhov[ll], A, rhov[jj])
+            Nm[jj, ll] = scal_prod(rhov[jj], rhov[ll])
+            Nm[ll, jj] = np.conj(Nm[jj, ll])
+    coef = scipy.linalg.expm(np.linalg.solve(Nm, Hm))[:, 0]
+    rhov[0] = compress_sum_var(rhov[0], coef, rhov, 1)
+    normalize_lo_(rhov[0])
+    return coef
+
+
 def compress_sum_var_apply_H_left_(A0, env, envop, Ain, coef, A, H):
     """src/compression.jl:889-944: stage with an R->L half sweep (coefficients in the right boundary)."""
     na = len(Ain)

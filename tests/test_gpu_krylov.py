@@ -1,0 +1,86 @@
+"""Full-sweep sum compressions and the Arnoldi step (the §f1 row) on the GPU against the oracle."""
+import numpy as np
+import pytest
+
+from gpu_util import fidelity, relerr
+from oracle import dense as D
+from oracle import models as OM
+from oracle import mps_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def _sites_close(gpu_mps, ref_sites, tol):
+    for k, (a, b) in enumerate(zip(gpu_mps.sites(), ref_sites)):
+        assert relerr(a, b) < tol, "site %d: %.3e" % (k, relerr(a, b))
+
+
+def _randoms(na, chi, d, n, seed):
+    rng = np.random.default_rng(seed)
+    out = [R.mpsrandom(na, chi, d, rng) for _ in range(n)]
+    return [m for m, _ in out], out[0][1]
+
+
+@pytest.mark.parametrize("sweeps", [1, 2])
+def test_compress_sum_var_apply_H_full_sweeps(gpu_ctx, sweeps):
+    """compress_sum_var_apply_H! (src/compression.jl:805-887): two plain terms + H term."""
+    import mpsb200 as K
+    na, chi = 8, 8
+    terms, dims = _randoms(na, chi, 2, 4, 31)
+    p = OM.SpinChain(na, omega=0.5)
+    H = OM.sm_hamiltonian(p, 0.5, 0.05, 0.0)
+    wl = [1] + [4] * (na - 1) + [1]
+    coef = [0.4 - 0.1j, -0.3j, 1.0]
+    A0 = R.copy_mps(terms[3])
+    eop = R.build_env(dims, dims, wl)
+    R.compress_sum_var_apply_H_(A0, eop, coef, terms[:3], H, sweeps)
+    g = [K.MPS.from_sites(t, gpu_ctx) for t in terms]
+    gA0 = g[3].clone()
+    geop = K.build_env(dims, dims, wl, gpu_ctx)
+    K.compress_sum_var_apply_H_(gA0, geop, coef, g[:3], K.MPO.from_sites(H, gpu_ctx), sweeps)
+    _sites_close(gA0, A0, 1e-10)
+
+
+def test_compress_sum_var(gpu_ctx):
+    """compress_sum_var (src/compression.jl:496-565): three plain terms, guess = first term."""
+    import mpsb200 as K
+    na, chi = 9, 8
+    terms, dims = _randoms(na, chi, 2, 3, 32)
+    coef = [0.3 - 0.2j, 1.1, -0.7j]
+    ref = R.compress_sum_var(R.copy_mps(terms[0]), coef, terms, 1)
+    g = [K.MPS.from_sites(t, gpu_ctx) for t in terms]
+    out = K.compress_sum_var(g[0], coef, g, 1)
+    _sites_close(out, ref, 1e-10)
+    with pytest.raises(K.MpsbError):   # the output must not be one of the terms
+        from mpsb200 import _lib
+        import ctypes as C
+        cb = np.asarray(coef, dtype=np.complex128).view(np.float64)
+        arr = (C.c_void_p * 3)(*[m.h.value for m in g])
+        _lib.call("mpsb_compress_sum_var", gpu_ctx.h, g[0].h, g[0].h,
+                  cb.ctypes.data_as(C.POINTER(C.c_double)), 3, arr, 1)
+
+
+@pytest.mark.parametrize("na,chi,numv", [(8, 16, 4), (10, 8, 3)])
+def test_arnoldi_expm_matches_oracle(gpu_ctx, na, chi, numv):
+    """Arnoldi_expm! (src/timeevolution.jl:88-119): Krylov coefficients and the new state."""
+    import mpsb200 as K
+    dt = 0.02
+    p = OM.SpinChain(na, omega=0.5)
+    A = OM.sm_hamiltonian(p, 0, dt, 0.0)
+    rng = np.random.default_rng(33)
+    psi, dims = R.mpsrandom(na, chi, 2, rng)
+    R.normalize_lo_(psi)
+    wl = [1] + [4] * (na - 1) + [1]
+    rhov = [R.copy_mps(psi) for _ in range(numv)]
+    coef = R.Arnoldi_expm_(A, rhov, numv, None, R.build_env(dims, dims, wl))
+    gpsi = K.MPS.from_sites(psi, gpu_ctx)
+    grhov = [gpsi.clone() for _ in range(numv)]
+    gcoef = K.Arnoldi_expm_(K.MPO.from_sites(A, gpu_ctx), grhov, numv, None,
+                            K.build_env(dims, dims, wl, gpu_ctx))
+    assert np.abs(np.asarray(gcoef) - coef).max() < 1e-10
+    got, want = grhov[0].sites(), rhov[0]
+    if chi >= 2 ** (na // 2):   # full bond dimension: the states themselves
+        assert np.abs(D.mps_to_dense(got) - D.mps_to_dense(want)).max() < 1e-10
+    else:
+        _sites_close(grhov[0], want, 1e-9)
+    assert 1 - fidelity(got, want) < 1e-12

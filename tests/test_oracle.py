@@ -205,3 +205,64 @@ def test_trajectory_runs_and_normalises(seed):
     rec = DR.run_trajectory(p, 8, 0.01, 30, r1, r2, measure_int=10)
     assert abs(R.norm_lo(rec["A"]) - 1) < 1e-12
     assert rec["e_pop"].shape == (4, 8)
+
+
+def _arnoldi_dense(Ad, v0, numv):
+    """Arnoldi_expm! (src/timeevolution.jl:88-119) restated on dense vectors, with the
+    reference's own scalar conventions: scal_op_prod(m1, A, m2) = conj(<m1|A|m2>) (its left
+    environments are stored conjugated, update_le = AOL' * A0, src/mps_base.jl:223-231) and
+    scal_prod(m1, m2) = <m1|m2>."""
+    import scipy.linalg
+    sop = lambda a, b: np.conj(np.vdot(a, Ad @ b))
+    v = [v0 / np.linalg.norm(v0)]
+    Nm = np.eye(numv, dtype=complex)
+    Hm = np.zeros((numv, numv), dtype=complex)
+    Hm[0, 0] = sop(v[0], v[0])
+    for jj in range(1, numv):
+        w = Ad @ v[jj - 1] - sum(Hm[ll, jj - 1] * v[ll] for ll in range(jj))
+        v.append(w / np.linalg.norm(w))
+        Hm[jj, jj] = sop(v[jj], v[jj])
+        for ll in range(jj):
+            Hm[jj, ll] = sop(v[jj], v[ll])
+            Hm[ll, jj] = sop(v[ll], v[jj])
+            Nm[jj, ll] = np.vdot(v[jj], v[ll])
+            Nm[ll, jj] = np.conj(Nm[jj, ll])
+    coef = scipy.linalg.expm(np.linalg.solve(Nm, Hm))[:, 0]
+    out = sum(c * x for c, x in zip(coef, v))
+    return out / np.linalg.norm(out), coef
+
+
+def test_arnoldi_expm_full_bond_matches_dense_restatement():
+    """At full bond dimension every compression is exact, so the MPS Arnoldi step equals the
+    same algorithm on dense vectors.  (Because scal_op_prod returns the conjugate matrix
+    element, the reference's step is exp(A) psi only to first order in A for a general A.)"""
+    import scipy.linalg
+    na, dt = 5, 0.01
+    p = M.SpinChain(na, omega=0.5)
+    A = M.sm_hamiltonian(p, 0, dt, 0.0)
+    Ad = D.mpo_to_dense(A)
+    rng = np.random.default_rng(3)
+    psi, dims = R.mpsrandom(na, 8, 2, rng)
+    R.normalize_lo_(psi)
+    for numv in (2, 4):
+        rhov = [R.copy_mps(psi) for _ in range(numv)]
+        envop = R.build_env(dims, dims, [1] + [4] * (na - 1) + [1])
+        coef = R.Arnoldi_expm_(A, rhov, numv, None, envop)
+        want, wcoef = _arnoldi_dense(Ad, D.mps_to_dense(psi), numv)
+        got = D.mps_to_dense(rhov[0])
+        assert np.abs(coef - wcoef).max() < 1e-10
+        assert abs(np.linalg.norm(got) - 1) < 1e-12
+        assert 1 - abs(np.vdot(want, got)) < 1e-12
+        exact = scipy.linalg.expm(Ad) @ D.mps_to_dense(psi)
+        assert 1 - abs(np.vdot(exact / np.linalg.norm(exact), got)) < 1e-2   # agrees to O(|A|) only
+
+
+def test_compress_sum_var_full_bond_is_exact():
+    """compress_sum_var (src/compression.jl:496-565) at full bond dimension reproduces the sum."""
+    na = 5
+    rng = np.random.default_rng(4)
+    terms = [R.mpsrandom(na, 8, 2, rng)[0] for _ in range(3)]
+    coef = [0.3 - 0.2j, 1.1, -0.7j]
+    out = R.compress_sum_var(R.copy_mps(terms[0]), coef, terms, 1)
+    want = sum(c * D.mps_to_dense(t) for c, t in zip(coef, terms))
+    assert np.abs(D.mps_to_dense(out) - want).max() < 1e-12
