@@ -502,7 +502,7 @@ size_t layout(QrParams& P, int n, int C, int rows, int nb) {
 // memory one panel ahead (cp.async, double-buffered); the panels' T_p are staged once.
 constexpr int TR_WARPS = 8;
 
-template <int QMAX>
+template <int QMAX, bool STAGE>
 __global__ void __launch_bounds__(32 * TR_WARPS) qr_tmat_kernel(int m, int n, int nb, const cd* __restrict__ Vg,
                                                                  const cd* __restrict__ Tg,
                                                                  const cd* __restrict__ Gg, cd* __restrict__ Mg) {
@@ -528,6 +528,7 @@ __global__ void __launch_bounds__(32 * TR_WARPS) qr_tmat_kernel(int m, int n, in
     for (int i = (c / nb + 1) * nb + lane; i < n; i += 32) M[i + (int64_t)c * n] = cmk(0.0, 0.0);
 
   auto stage = [&](int pi, int buf) {   // G[r, p0 + j], r < p0, j < pw
+    if constexpr (!STAGE) return;
     const int p0 = pi * nb, pw = min(nb, n - p0);
     cd* dst = Gs + buf * nb * n;
     for (int e = threadIdx.x; e < pw * p0; e += blockDim.x) {
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(32 * TR_WARPS) qr_tmat_kernel(int m, int n, in
     asm volatile("cp.async.commit_group;\n" ::);
   };
   const int pstart = ctop / nb;
-  for (int e = threadIdx.x; e < (pstart + 1) * nb * nb; e += blockDim.x) {   // T of panels 0 .. pstart
+  for (int e = threadIdx.x; STAGE && e < (pstart + 1) * nb * nb; e += blockDim.x) {   // T of panels 0 .. pstart
     const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(Ts + e));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(T + e));
   }
@@ -547,9 +548,9 @@ __global__ void __launch_bounds__(32 * TR_WARPS) qr_tmat_kernel(int m, int n, in
     const int k = pstart - pi;
     if (pi > 0) {
       stage(pi - 1, (k + 1) & 1);
-      asm volatile("cp.async.wait_group 1;\n" ::);
+      if constexpr (STAGE) asm volatile("cp.async.wait_group 1;\n" ::);
     } else {
-      asm volatile("cp.async.wait_group 0;\n" ::);
+      if constexpr (STAGE) asm volatile("cp.async.wait_group 0;\n" ::);
     }
     __syncthreads();
     const int p0 = pi * nb, pw = min(nb, n - p0);
@@ -559,7 +560,7 @@ __global__ void __launch_bounds__(32 * TR_WARPS) qr_tmat_kernel(int m, int n, in
 #pragma unroll
       for (int q = 0; q < QMAX; ++q)
         if (q == qb) yb = y[q];
-      const cd* Tp = Ts + pi * nb * nb;
+      const cd* Tp = STAGE ? Ts + pi * nb * nb : T + (int64_t)pi * nb * nb;
       cd a0 = cmk(0.0, 0.0), a1 = cmk(0.0, 0.0);
       for (int jj = 0; jj < pw; ++jj) {
         const cd rj = cmk(__shfl_sync(0xffffffffu, yb.x, base + jj), __shfl_sync(0xffffffffu, yb.y, base + jj));
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(32 * TR_WARPS) qr_tmat_kernel(int m, int n, in
       const cd* Gc = Gs + (k & 1) * nb * n;
       for (int jj = 0; jj < pw; ++jj) {
         const cd mj = cmk(__shfl_sync(0xffffffffu, mi.x, base + jj), __shfl_sync(0xffffffffu, mi.y, base + jj));
-        const cd* gcol = Gc + jj * n;
+        const cd* gcol = STAGE ? Gc + jj * n : G + (int64_t)(p0 + jj) * n;
 #pragma unroll
         for (int q = 0; q < QMAX; ++q) {
           const int r = lane + 32 * q;
@@ -584,16 +585,22 @@ __global__ void __launch_bounds__(32 * TR_WARPS) qr_tmat_kernel(int m, int n, in
 
 typedef void (*TmatKernel)(int, int, int, const cd*, const cd*, const cd*, cd*);
 
-TmatKernel tmat_kernel_for(int n) {
-  if (n <= 32) return qr_tmat_kernel<1>;
-  if (n <= 64) return qr_tmat_kernel<2>;
-  if (n <= 128) return qr_tmat_kernel<4>;
-  if (n <= 256) return qr_tmat_kernel<8>;
-  if (n <= 512) return qr_tmat_kernel<16>;
+size_t tmat_smem(int n, int nb) { return (2 * (size_t)nb * n + (size_t)((n + nb - 1) / nb) * nb * nb) * sizeof(cd); }
+
+// The staged variant when G's panel columns (double-buffered) and every T_p fit in shared
+// memory, else the same algorithm reading them from global memory (L2).
+template <bool ST>
+TmatKernel tmat_pick(int n) {
+  if (n <= 32) return qr_tmat_kernel<1, ST>;
+  if (n <= 64) return qr_tmat_kernel<2, ST>;
+  if (n <= 128) return qr_tmat_kernel<4, ST>;
+  if (n <= 256) return qr_tmat_kernel<8, ST>;
+  if (n <= 512) return qr_tmat_kernel<16, ST>;
   return nullptr;
 }
-
-size_t tmat_smem(int n, int nb) { return (2 * (size_t)nb * n + (size_t)((n + nb - 1) / nb) * nb * nb) * sizeof(cd); }
+TmatKernel tmat_kernel_for(int n, int nb) {
+  return tmat_smem(n, nb) <= SMEM_LIMIT ? tmat_pick<true>(n) : tmat_pick<false>(n);
+}
 
 struct Choice {
   int C = 0, rpl = 0, nb = 0;
@@ -616,7 +623,7 @@ bool choose(int m, int n, Choice& ch) {
     if (C > CMAX) continue;
     for (int nb : {16, 8, 4}) {
       size_t b = layout(P, n, C, rows, nb);
-      if (b <= SMEM_LIMIT && tmat_smem(n, nb) <= SMEM_LIMIT && n <= 512) {
+      if (b <= SMEM_LIMIT) {
         ch.C = C; ch.rpl = rpl; ch.nb = nb; ch.smem = b;
         return true;
       }
@@ -625,35 +632,36 @@ bool choose(int m, int n, Choice& ch) {
   return false;
 }
 
-}  // namespace
-
-bool qr_supported(int m, int n) {
-  Choice ch;
-  return m >= n && n >= 1 && choose(m, n, ch);
+// Strided m x n matrix fill: COPY dst = src, UPPER dst = triu(src), IDENT dst = [I; 0].
+enum { MAT_COPY = 0, MAT_UPPER, MAT_IDENT };
+__global__ void mat_kernel(int mode, int m, int n, const cd* __restrict__ src, int64_t sr, int64_t sc, cd* dst,
+                           int64_t dr, int64_t dc) {
+  const int64_t total = (int64_t)m * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int g = (int)(e % m), k = (int)(e / m);
+    cd v;
+    if (mode == MAT_IDENT) v = cmk(g == k ? 1.0 : 0.0, 0.0);
+    else if (mode == MAT_UPPER && k < g) v = cmk(0.0, 0.0);
+    else v = src[g * sr + k * sc];
+    dst[g * dr + k * dc] = v;
+  }
 }
 
-int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s) {
-  if (p.m < p.n || p.n < 1 || p.batch < 1) return MPSB_ERR_DIMENSION;
-  if (p.batch > 65535) return MPSB_ERR_UNSUPPORTED;
-  if (!ws) return MPSB_ERR_INVALID_ARG;
-  Choice ch;
-  const TmatKernel tk = tmat_kernel_for(p.n);
-  if (!choose(p.m, p.n, ch) || !tk) {
-    set_last_message("QR of a %d x %d matrix exceeds the cluster shared-memory capacity", p.m, p.n);
-    return MPSB_ERR_UNSUPPORTED;
-  }
-  const int m = p.m, n = p.n, nb = ch.nb, npan = (n + nb - 1) / nb;
-  // scratch: V [batch][n][m], the panels' T [batch][npan][nb][nb], G = V^H V and
-  // M = T V1^H [batch][n][n] each
-  const size_t nV = (size_t)p.batch * m * n, nT = (size_t)p.batch * npan * nb * nb, nG = (size_t)p.batch * n * n;
-  MPSB_TRY(devbuf_ensure(ws, ws->qr, (nV + nT + 2 * nG) * sizeof(cd)));
-  cd* Vb = static_cast<cd*>(ws->qr.p);
-  cd* Tb = Vb + nV;
-  cd* Gb = Tb + nT;
-  cd* Mb = Gb + nG;
+int mat_launch(int mode, int m, int n, const cd* src, int64_t sr, int64_t sc, cd* dst, int64_t dr, int64_t dc,
+               Workspace* ws, cudaStream_t s) {
+  count_launch(ws);
+  const int64_t total = (int64_t)m * n;
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
+  mat_kernel<<<blocks, 256, 0, s>>>(mode, m, n, src, sr, sc, dst, dr, dc);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  return MPSB_OK;
+}
 
+// The cluster factorisation of every problem of p: R (if requested), the explicit reflectors
+// V [batch][n][m], the panels' T [batch][npanels][nb][nb], and E = [I; 0] in p.Q.
+int launch_factor(const QrProblem& p, const Choice& ch, cd* Vb, cd* Tb, cudaStream_t s) {
   QrParams P;
-  layout(P, n, ch.C, 32 * ch.rpl, ch.nb);
+  layout(P, p.n, ch.C, 32 * ch.rpl, ch.nb);
   P.p = p;
   P.V = Vb;
   P.Tg = Tb;
@@ -679,7 +687,15 @@ int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   MPSB_CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, P));
+  return MPSB_OK;
+}
 
+// Q = E - V (T V1^H) for every problem of p, p.Q holding E: G = V^H V, the back substitution
+// for M = T V1^H, and Q -= V M.
+int form_q(const QrProblem& p, int nb, const cd* Vb, const cd* Tb, cd* Gb, cd* Mb, Workspace* ws, cudaStream_t s) {
+  const int m = p.m, n = p.n;
+  const TmatKernel tk = tmat_kernel_for(n, nb);
+  if (!tk) return MPSB_ERR_UNSUPPORTED;
   const cd one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0), mone = cmk(-1.0, 0.0);
   {  // G = V^H V
     Gemm g;
@@ -691,18 +707,13 @@ int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s) {
     MPSB_TRY(gemm_launch(g, ws, s));
   }
   {  // M = T V1^H
-    const size_t smem = tmat_smem(n, nb);
-    static bool tattr[5] = {};
-    const int ti = n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : n <= 256 ? 3 : 4;
-    if (!tattr[ti]) {
-      MPSB_CUDA_TRY(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT));
-      tattr[ti] = true;
-    }
+    const size_t smem = tmat_smem(n, nb) <= SMEM_LIMIT ? tmat_smem(n, nb) : 0;
+    if (smem) MPSB_CUDA_TRY(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT));
     count_launch(ws);
     tk<<<dim3((n + TR_WARPS - 1) / TR_WARPS, p.batch), 32 * TR_WARPS, smem, s>>>(m, n, nb, Vb, Tb, Gb, Mb);
     MPSB_CUDA_TRY(cudaGetLastError());
   }
-  {  // Q = E - V M  (Q holds E)
+  {  // Q = E - V M
     Gemm g;
     g.M = m; g.N = n; g.K = n; g.batch = p.batch;
     g.A = Vb; g.a_m = 1; g.a_k = m; g.a_b = (int64_t)m * n;
@@ -712,6 +723,123 @@ int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s) {
     MPSB_TRY(gemm_launch(g, ws, s));
   }
   return MPSB_OK;
+}
+
+// Blocked QR for one matrix beyond the cluster's shared memory (for example 2048 x 512): the
+// working matrix is p.Q (X copied in unless they coincide); every 16-column panel is
+// factored by the cluster kernel (its R rows written back in place, its reflectors and T
+// kept), the trailing columns get A -= V (T^H (V^H A)) by three tensor-core GEMMs, and Q is
+// formed from all reflectors as in the single-kernel path.
+constexpr int BP = 16;
+
+int qr_blocked(const QrProblem& p, Workspace* ws, cudaStream_t s) {
+  const int m = p.m, n = p.n, npan = (n + BP - 1) / BP;
+  const int64_t qr_ = p.q_r, qc = p.q_c;
+  // scratch: V [n][m], T [npan][16][16], G and M [n][n], panel V and E [16][m], W and W2 [n][16]
+  const size_t nV = (size_t)m * n, nT = (size_t)npan * BP * BP, nG = (size_t)n * n, nP = (size_t)m * BP,
+               nW = (size_t)n * BP;
+  MPSB_TRY(devbuf_ensure(ws, ws->qr, (nV + nT + 2 * nG + 2 * nP + 2 * nW) * sizeof(cd)));
+  cd* Vb = static_cast<cd*>(ws->qr.p);
+  cd* Tb = Vb + nV;
+  cd* Gb = Tb + nT;
+  cd* Mb = Gb + nG;
+  cd* Vp = Mb + nG;
+  cd* Ep = Vp + nP;
+  cd* Wb = Ep + nP;
+  cd* W2 = Wb + nW;
+  cd* A = p.Q;
+  if (p.X != p.Q || p.x_r != qr_ || p.x_c != qc)
+    MPSB_TRY(mat_launch(MAT_COPY, m, n, p.X, p.x_r, p.x_c, A, qr_, qc, ws, s));
+  MPSB_CUDA_TRY(cudaMemsetAsync(Vb, 0, nV * sizeof(cd), s));
+  const cd one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0), mone = cmk(-1.0, 0.0);
+  for (int pi = 0; pi < npan; ++pi) {
+    const int p0 = pi * BP, pw = std::min(BP, n - p0), mp = m - p0, nt = n - p0 - pw;
+    Choice ch;
+    if (!choose(mp, pw, ch) || ch.nb != BP) {
+      set_last_message("QR panel of %d x %d does not fit the cluster kernel", mp, pw);
+      return MPSB_ERR_UNSUPPORTED;
+    }
+    cd* Ap = A + p0 * qr_ + p0 * qc;
+    QrProblem pp;
+    pp.m = mp; pp.n = pw; pp.batch = 1;
+    pp.X = Ap; pp.x_r = qr_; pp.x_c = qc;
+    pp.Q = Ep; pp.q_r = 1; pp.q_c = mp;
+    pp.R = Ap; pp.r_r = qr_; pp.r_c = qc;   // R rows back in place (the panel's V is kept apart)
+    pp.err = p.err;
+    count_launch(ws);
+    MPSB_TRY(launch_factor(pp, ch, Vp, Tb + (int64_t)pi * BP * BP, s));
+    MPSB_CUDA_TRY(cudaMemcpy2DAsync(Vb + p0 + (int64_t)p0 * m, (size_t)m * sizeof(cd), Vp, (size_t)mp * sizeof(cd),
+                                    (size_t)mp * sizeof(cd), pw, cudaMemcpyDeviceToDevice, s));
+    if (nt <= 0) continue;
+    cd* At = A + p0 * qr_ + (int64_t)(p0 + pw) * qc;
+    {  // W = V^H A_trail
+      Gemm g;
+      g.M = pw; g.N = nt; g.K = mp;
+      g.A = Vp; g.a_m = mp; g.a_k = 1; g.conjA = true;
+      g.B = At; g.b_k = qr_; g.b_n = qc;
+      g.C = Wb; g.c_m = 1; g.c_n = BP;
+      g.alpha = one; g.beta = zero;
+      MPSB_TRY(gemm_launch(g, ws, s));
+    }
+    {  // W2 = T^H W
+      Gemm g;
+      g.M = pw; g.N = nt; g.K = pw;
+      g.A = Tb + (int64_t)pi * BP * BP; g.a_m = BP; g.a_k = 1; g.conjA = true;
+      g.B = Wb; g.b_k = 1; g.b_n = BP;
+      g.C = W2; g.c_m = 1; g.c_n = BP;
+      g.alpha = one; g.beta = zero;
+      MPSB_TRY(gemm_launch(g, ws, s));
+    }
+    {  // A_trail -= V W2
+      Gemm g;
+      g.M = mp; g.N = nt; g.K = pw;
+      g.A = Vp; g.a_m = 1; g.a_k = mp;
+      g.B = W2; g.b_k = 1; g.b_n = BP;
+      g.C = At; g.c_m = qr_; g.c_n = qc;
+      g.alpha = mone; g.beta = one;
+      MPSB_TRY(gemm_launch(g, ws, s));
+    }
+  }
+  if (p.R) MPSB_TRY(mat_launch(MAT_UPPER, n, n, A, qr_, qc, p.R, p.r_r, p.r_c, ws, s));
+  MPSB_TRY(mat_launch(MAT_IDENT, m, n, nullptr, 0, 0, A, qr_, qc, ws, s));
+  QrProblem q = p;
+  return form_q(q, BP, Vb, Tb, Gb, Mb, ws, s);
+}
+
+bool blocked_ok(int m, int n) {
+  Choice ch;
+  return n <= 512 && choose(m, std::min(n, BP), ch) && ch.nb == BP;
+}
+
+}  // namespace
+
+bool qr_supported(int m, int n) {
+  Choice ch;
+  return m >= n && n >= 1 && n <= 512 && (choose(m, n, ch) || blocked_ok(m, n));
+}
+
+int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s) {
+  if (p.m < p.n || p.n < 1 || p.batch < 1) return MPSB_ERR_DIMENSION;
+  if (p.batch > 65535) return MPSB_ERR_UNSUPPORTED;
+  if (!ws) return MPSB_ERR_INVALID_ARG;
+  const int m = p.m, n = p.n;
+  Choice ch;
+  if (n > 512 || (!choose(m, n, ch) && (p.batch != 1 || !blocked_ok(m, n)))) {
+    set_last_message("QR of a %d x %d matrix (batch %d) is beyond the supported shapes", m, n, p.batch);
+    return MPSB_ERR_UNSUPPORTED;
+  }
+  if (!choose(m, n, ch)) return qr_blocked(p, ws, s);
+  const int nb = ch.nb, npan = (n + nb - 1) / nb;
+  // scratch: V [batch][n][m], the panels' T [batch][npan][nb][nb], G = V^H V and
+  // M = T V1^H [batch][n][n] each
+  const size_t nV = (size_t)p.batch * m * n, nT = (size_t)p.batch * npan * nb * nb, nG = (size_t)p.batch * n * n;
+  MPSB_TRY(devbuf_ensure(ws, ws->qr, (nV + nT + 2 * nG) * sizeof(cd)));
+  cd* Vb = static_cast<cd*>(ws->qr.p);
+  cd* Tb = Vb + nV;
+  cd* Gb = Tb + nT;
+  cd* Mb = Gb + nG;
+  MPSB_TRY(launch_factor(p, ch, Vb, Tb, s));
+  return form_q(p, nb, Vb, Tb, Gb, Mb, ws, s);
 }
 
 }  // namespace mpsb

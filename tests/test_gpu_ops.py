@@ -65,6 +65,37 @@ def test_qr_mixed_exact_zero_columns(gpu_ctx):
     assert np.abs(Q.conj().T @ Q - np.eye(24)).max() < 1e-12
 
 
+@pytest.mark.parametrize("m,n", [(2048, 512), (1024, 300), (640, 40)])
+def test_qr_blocked_path_matches_lapack(gpu_ctx, m, n):
+    """Shapes beyond one cluster's shared memory (2048 x 512 is the interior site of a
+    chi = 512, d = 4 chain): panel-by-panel factorisation with GEMM trailing updates."""
+    rng = np.random.default_rng(m + n)
+    X = crand(rng, m, n)
+    q_ref, r_ref = R.julia_qr(X)
+    dX, dQ, dR = to_dev(X), empty_dev((m, n)), empty_dev((n, n))
+    _call(gpu_ctx, "mpsb_op_qr", _p(dX), _p(dQ), _p(dR), m, n)
+    Q, Rr = from_dev(dQ, (m, n)), from_dev(dR, (n, n))
+    assert relerr(Q, q_ref) < 1e-10
+    assert relerr(Rr, r_ref) < 1e-10
+    assert np.abs(Q.conj().T @ Q - np.eye(n)).max() < 1e-12
+    assert np.abs(from_dev(dX, (m, n)) - X).max() == 0      # the input is left untouched
+    dX2 = to_dev(X)                                            # in place
+    _call(gpu_ctx, "mpsb_op_qr", _p(dX2), _p(dX2), None, m, n)
+    assert np.abs(from_dev(dX2, (m, n)) - Q).max() < 1e-13
+
+
+def test_qr_blocked_rank_deficient_padded_site(gpu_ctx):
+    """A zero-padded product site at chi = 512, d = 4 (tau = 0 and junk columns) on the blocked path."""
+    dl, d, dr = 512, 4, 512
+    X = np.zeros((dl * d, dr), dtype=np.complex128)
+    X[1, 0] = 1.0
+    q_ref = R.qrq(X)
+    dX = to_dev(X)
+    _call(gpu_ctx, "mpsb_op_qr", _p(dX), _p(dX), None, dl * d, dr)
+    Q = from_dev(dX, (dl * d, dr))
+    assert np.abs(Q - q_ref).max() < 1e-12
+
+
 SHAPES = [  # chiL, d, chiR, wL, wR, chi0
     (1, 2, 2, 1, 4, 2), (4, 2, 8, 4, 4, 8), (32, 2, 32, 4, 4, 32), (17, 3, 29, 5, 3, 23),
     (128, 4, 128, 8, 8, 128), (64, 4, 128, 6, 6, 100),
