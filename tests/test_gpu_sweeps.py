@@ -214,3 +214,33 @@ def test_graph_replay_is_bitwise_eager(gpu_ctx):
         outs.append(np.concatenate([s.ravel() for s in b.A.sites()]))
     gpu_ctx.set_graphs(True)
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_rk4_rho_chi512_blocked_qr(gpu_ctx):
+    """The chi <= 512 configuration at reduced length (N=10, d=4, w=8): a random chi=64 state
+    (mpsrandom semantics, normalised) expanded to chi=512; its 1024 x 512 and 2048 x 256 QRs
+    take the blocked path inside expandmps and every sweep.  One 11-argument RK4 step against
+    the oracle, through gauge-invariant quantities (the padded bonds are rank-deficient)."""
+    import mpsb200 as K
+    na, chi, dt = 10, 512, 0.005
+    rng = np.random.default_rng(60)
+    r64, _ = R.mpsrandom(na, 64, 4, rng)
+    R.normalize_lo_(r64)
+    rho, dims = R.expandmps(r64, chi)
+    g, gdims = K.expandmps(K.MPS.from_sites(r64, gpu_ctx), chi)
+    assert list(gdims) == list(dims)
+    assert 1 - fidelity(g.sites(), rho) < 1e-12
+    p = OM.SpinChain(na, gam_eg=0.1, omega=0.5, gam_phi=0.1)
+    L = [OM.construct_L_spin_model(p, 1, dt / 2, 0, 8), OM.construct_L_spin_model(p, 0, 1, dt / 2, 8),
+         OM.construct_L_spin_model(p, 1, dt / 2, dt, 8)]
+    wl = [1] + [8] * (na - 1) + [1]
+    A0, A1, A2, A3 = (R.copy_mps(rho) for _ in range(4))
+    e = [R.build_env(dims, dims) for _ in range(3)]
+    R.RK4stp_apply_H_half_(dt, L, A0, rho, A1, A2, A3, *e, R.build_env(dims, dims, wl))
+    g0, g1, g2, g3 = (g.clone() for _ in range(4))
+    ge = [K.build_env(dims, dims, None, gpu_ctx) for _ in range(3)]
+    K.RK4stp_apply_H_half_(dt, [K.MPO.from_sites(l, gpu_ctx) for l in L], g0, g, g1, g2, g3, *ge,
+                           K.build_env(dims, dims, wl, gpu_ctx))
+    got = g0.sites()
+    assert abs(R.scal_prod(got, got) / R.scal_prod(A0, A0) - 1) < 1e-10
+    assert 1 - fidelity(got, A0) < 1e-10
