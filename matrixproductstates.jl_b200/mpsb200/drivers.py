@@ -7,6 +7,8 @@ Every tensor operation is a libmpsb200 call; the host only makes the jump decisi
 FP64 probabilities the device returns (``r1``/``r2`` uniforms are injected by the caller, the
 stand-in for Julia's ``srand(setrand); rand(tstep)`` stream).
 """
+import os
+
 import numpy as np
 
 from . import core as K
@@ -117,11 +119,38 @@ class DensityBuffers:
         return tr, see, np.array(spm)
 
 
-def run_density(p, dmax, dt, nsteps, w=6, measure_int=10, pairs=((0, 1),), ctx=None, rho=None):
+def run_density(p, dmax, dt, nsteps, w=6, measure_int=10, pairs=((0, 1),), ctx=None, rho=None,
+                checkpoint=None, checkpoint_int=0):
+    """The density-matrix time loop (examples/spin_model_density_matrix.jl): nsteps in-place RK4
+    steps with (Tr rho, <see_i>, <s+_i s-_j>) every measure_int steps.
+
+    With `checkpoint` (a file path) the run restarts from that file when it exists -- rho and
+    the step index i_last, as the reference's restart example reads them -- and rewrites it
+    every `checkpoint_int` steps (0: only at the end)."""
+    from . import checkpoint as CK
+    i0, obs = 0, None
+    if checkpoint and os.path.exists(checkpoint):
+        st = CK.read_data_file(checkpoint, ctx)
+        if abs(float(st["dt"]) - dt) > 0 or int(st["d_max"]) != dmax or int(st["measure_int"]) != measure_int:
+            raise ValueError("checkpoint %s was written with other dt / d_max / measure_int" % checkpoint)
+        rho, i0 = st["rho"], int(st["i_last"])
+        obs = [(t, s_, m_) for t, s_, m_ in zip(st["tr_rho"], st["see"], st["spm"])]
     b = DensityBuffers(p, dmax, dt, w, ctx, rho)
-    obs = [b.observables(pairs)]
-    for i in range(nsteps):
+    if obs is None:
+        obs = [b.observables(pairs)]
+
+    def save(i):
+        CK.write_data_file(checkpoint, {
+            "rho": b.rho, "i_last": i, "dt": dt, "d_max": dmax, "measure_int": measure_int, "na": p.na,
+            "tr_rho": np.array([o[0] for o in obs]), "see": np.array([o[1] for o in obs]),
+            "spm": np.array([o[2] for o in obs])})
+
+    for i in range(i0, nsteps):
         b.step()
         if (i + 1) % measure_int == 0:
             obs.append(b.observables(pairs))
+        if checkpoint and checkpoint_int and (i + 1) % checkpoint_int == 0 and i + 1 < nsteps:
+            save(i + 1)
+    if checkpoint:
+        save(nsteps)
     return b, obs

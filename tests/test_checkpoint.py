@@ -1,0 +1,39 @@
+"""Checkpoint / restart (the reference's restart example) : file format on the host, and a
+resumed density-matrix run on the GPU equal to an uninterrupted one."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mps_ref as R
+
+
+def test_checkpoint_round_trip_host(tmp_path):
+    from mpsb200 import checkpoint as CK
+    rng = np.random.default_rng(1)
+    sites, dims = R.mpsrandom(6, 8, 4, rng)
+    f = str(tmp_path / "run_temp.npz")
+    CK.write_data_file(f, {"rho": sites, "i_last": 17, "dt": 0.005, "tr_rho": np.array([1.0 + 0j, 0.99]),
+                           "rj": np.arange(6.0)})
+    st = CK.read_data_file(f, device=False)
+    assert st["i_last"] == 17 and st["dt"] == 0.005
+    assert np.array_equal(st["tr_rho"], [1.0 + 0j, 0.99]) and np.array_equal(st["rj"], np.arange(6.0))
+    assert len(st["rho"]) == 6 and all(np.array_equal(a, b) for a, b in zip(st["rho"], sites))
+    assert not os.path.exists(f + ".tmp")
+    with pytest.raises(ValueError):
+        CK.write_data_file(f, {"a/b": 1})
+
+
+@pytest.mark.gpu
+def test_resumed_density_run_equals_uninterrupted(gpu_ctx, tmp_path):
+    from mpsb200 import drivers as GDR, models as GM
+    na, chi, dt, n = 6, 16, 0.005, 8
+    pg = GM.WaveguideChain(na, gam_eg=0.1, omega=0.5, gam_phi=0.1)
+    b_ref, obs_ref = GDR.run_density(pg, chi, dt, n, w=8, measure_int=2, ctx=gpu_ctx)
+    f = str(tmp_path / "rho_temp.npz")
+    GDR.run_density(pg, chi, dt, 4, w=8, measure_int=2, ctx=gpu_ctx, checkpoint=f, checkpoint_int=4)
+    b, obs = GDR.run_density(pg, chi, dt, n, w=8, measure_int=2, ctx=gpu_ctx, checkpoint=f)
+    assert all(np.array_equal(a, c) for a, c in zip(b.rho.sites(), b_ref.rho.sites()))
+    assert len(obs) == len(obs_ref)
+    for (t, s, m), (tr, sr, mr) in zip(obs, obs_ref):
+        assert t == tr and np.array_equal(s, sr) and np.array_equal(m, mr)
