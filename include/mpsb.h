@@ -133,6 +133,17 @@ int mpsb_compress_sum_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, 
 int mpsb_compress_sum_var(mpsb_ctx* ctx, mpsb_mps* A0, const mpsb_mps* Ain, const double* coef,
                           int numv, mpsb_mps* const* A, int maxsweeps);
 
+/* ground_state_search!(At, H, maxsweeps, converge_rat, eigs_tol)  src/groundstate.jl:67-147
+ * Single-site sweeps (left na..2, right 1..na-1, then site na) replacing each site by the
+ * lowest eigenvector of its effective operator (A_prod_LOR_eigs, src/MatrixProductStates.jl:246-253)
+ * and re-orthogonalising with the QR the reference uses; stops after a sweep whose last
+ * eigenvalue has |ae| > converge_rat |ae at the sweep's first site| or |ae| < 1e-10.
+ * The reference's ARPACK eigs(which=:SR) is replaced by Lanczos (full reorthogonalisation,
+ * same tolerance rule); the eigenvector phase is fixed by <start|x> > 0.  *ae = last eigenvalue.
+ * steady_state_search! (src/steadystate.jl:6-86) is this call with the product MPO Lconj*L. */
+int mpsb_ground_state_search(mpsb_ctx* ctx, mpsb_mps* At, const mpsb_mpo* H, int maxsweeps,
+                             double converge_rat, double eigs_tol, double* ae);
+
 /* ---------------------------------------------------------------- gauge / norms
  * normalize_lo!(mps) src/orthonormalisation.jl:97-103 -> *no = sum(abs2, mps[end])
  * norm_lo(mps)       src/orthonormalisation.jl:117-121

@@ -410,6 +410,16 @@ int mpsb_compress_sum_var(mpsb_ctx* ctx, mpsb_mps* A0, const mpsb_mps* Ain, cons
   return full_sum_var(ctx, A0, nullptr, coef, numv, A, nullptr, maxsweeps);
 }
 
+int mpsb_ground_state_search(mpsb_ctx* ctx, mpsb_mps* At, const mpsb_mpo* H, int maxsweeps, double converge_rat,
+                             double eigs_tol, double* ae) {
+  MPSB_TRY(bind(ctx));
+  double e = 0.0;
+  MPSB_TRY(ground_state_search(ctx, At, H, maxsweeps, converge_rat, eigs_tol, &e));
+  MPSB_TRY(sync(ctx));
+  if (ae) *ae = e;
+  return MPSB_OK;
+}
+
 // ---------------------------------------------------------------- gauge / norms
 int mpsb_norm_lo(mpsb_ctx* ctx, const mpsb_mps* A, double* no) {
   MPSB_TRY(bind(ctx));

@@ -17,7 +17,7 @@ int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out) {
   return MPSB_OK;
 }
 
-static inline int run_gemm(mpsb_ctx* ctx, const Gemm& g) {
+int run_gemm(mpsb_ctx* ctx, const Gemm& g) {
   void* before = ctx->ws.splitk.p;
   int st = gemm_launch(g, &ctx->ws, ctx->stream);
   if (ctx->ws.splitk.p != before) ctx->ws_generation++;
@@ -196,7 +196,7 @@ static int same_dims(const mpsb_mps* a, const mpsb_mps* b) {
   return a && b && a->na == b->na && a->d == b->d && a->dims == b->dims;
 }
 
-static int set_boundary(mpsb_ctx* ctx, cd* p, cd v) {
+int set_boundary(mpsb_ctx* ctx, cd* p, cd v) {
   count_launch(&ctx->ws);
   return set_value(p, v, ctx->stream);
 }

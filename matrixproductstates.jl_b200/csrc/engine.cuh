@@ -71,7 +71,7 @@ namespace mpsb {
 // named scratch slots in Workspace::named
 enum Slot {
   SLOT_T = 0, SLOT_AOR, SLOT_G1, SLOT_AOL, SLOT_P0, SLOT_P1, SLOT_P2, SLOT_ENV0, SLOT_ENV1,
-  SLOT_MISC, SLOT_SUMENV, SLOT_COUNT
+  SLOT_MISC, SLOT_SUMENV, SLOT_GSENV, SLOT_GSVEC, SLOT_COUNT
 };
 
 int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out);
@@ -97,6 +97,8 @@ int op_update_renv(mpsb_ctx* ctx, const cd* A0, const cd* AR, cd* env, int chiA,
 int op_update_lenv(mpsb_ctx* ctx, const cd* A0, const cd* AL, cd* env, int lead, int chiR0, int y, bool conj);
 // QR of a site: left (reshape(A, Dl*d, Dr)) or right (transpose of reshape(A, Dl, d*Dr))
 int run_qr(mpsb_ctx* ctx, const QrProblem& p);
+int run_gemm(mpsb_ctx* ctx, const Gemm& g);
+int set_boundary(mpsb_ctx* ctx, cd* p, cd v);
 int op_orth_left(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr, cd* R /* Dr x Dr or null */);
 int op_orth_right(mpsb_ctx* ctx, cd* A, int Dl, int d, int Dr);
 
@@ -110,6 +112,8 @@ int compress_sum_var_full(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const cd
                           const mpsb_mps* const* A, const mpsb_mpo* H /* null: compress_sum_var */, int maxsweeps);
 int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain, const mpsb_mps* A,
                          const mpsb_mpo* H, int maxsweeps);
+int ground_state_search(mpsb_ctx* ctx, mpsb_mps* At, const mpsb_mpo* H, int maxsweeps, double converge_rat,
+                        double eigs_tol, double* ae);
 int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
              mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3, mpsb_env* env1,
              mpsb_env* env2, mpsb_env* env3, mpsb_env* envop);

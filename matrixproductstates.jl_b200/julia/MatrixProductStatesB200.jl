@@ -147,6 +147,15 @@ function compress_sum_var!(ctx::Ctx, A0::DMPS, Ain::DMPS, coef::Vector{<:Number}
         ctx.h, A0.h, Ain.h, c, length(c), hs, maxsweeps), :mpsb_compress_sum_var)
 end
 
+# ground_state_search!(At, H, maxsweeps, converge_rat, eigs_tol)   src/groundstate.jl:67-147
+function ground_state_search!(ctx::Ctx, At::DMPS, H::DMPO, maxsweeps::Integer, converge_rat::Real, eigs_tol::Real)
+    ae = Ref{Cdouble}(0)
+    check(ccall((:mpsb_ground_state_search, LIB), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cdouble, Cdouble, Ref{Cdouble}),
+                ctx.h, At.h, H.h, maxsweeps, converge_rat, eigs_tol, ae), :mpsb_ground_state_search)
+    return ae[]
+end
+
 # normalize_lo!(mps)   src/orthonormalisation.jl:97-103
 function normalize_lo!(ctx::Ctx, A::DMPS)
     no = Ref{Cdouble}(0)

@@ -8,7 +8,8 @@ from .core import (  # noqa: F401
     MPO, MPS, Arnoldi_expm_, Context, Env, RK4stp_apply_H_half_, apply_site_operator_, applyMPOtoMPS,
     build_env, compress_sum_var, compress_sum_var_apply_H_, compress_sum_var_apply_H_left_,
     compress_sum_var_apply_H_right_, compress_var_apply_H_,
-    compress_var_apply_H_left_, default_context, expandmps, leftorth_sites_, leftorthogonalizeQR_,
+    compress_var_apply_H_left_, default_context, expandmps, ground_state_search_, leftorth_sites_,
+    leftorthogonalizeQR_, product_mpo, steady_state_search_,
     leftorthonormalizationQR_, makemps, makempo, measure_local, mpsgroundstate, mpsproductstate,
     mpsrandom, norm_lo, normalize_lo_, scal_op_prod, scal_prod, scal_prod_no_conj,
 )

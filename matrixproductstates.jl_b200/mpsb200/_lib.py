@@ -58,6 +58,7 @@ SIGNATURES = {
     "mpsb_compress_var_apply_H": ([_vp] * 6 + [_i], _i),
     "mpsb_compress_sum_var_apply_H": ([_vp, _vp, _vp, _pd, _i, _pvp, _vp, _i], _i),
     "mpsb_compress_sum_var": ([_vp, _vp, _vp, _pd, _i, _pvp, _i], _i),
+    "mpsb_ground_state_search": ([_vp, _vp, _vp, _i, _d, _d, _pd], _i),
     "mpsb_normalize_lo": ([_vp, _vp, _pd], _i),
     "mpsb_norm_lo": ([_vp, _vp, _pd], _i),
     "mpsb_leftorthonormalizationQR": ([_vp, _vp, _pd], _i),

@@ -435,6 +435,34 @@ def Arnoldi_expm_(A, rhov, numv, env, envop):
     return coef
 
 
+def ground_state_search_(At, H, maxsweeps, converge_rat, eigs_tol):
+    """src/groundstate.jl:67-147: At (left canonical guess) <- single-site ground-state sweeps
+    of the MPO H; returns the last local eigenvalue."""
+    ae = C.c_double()
+    _lib.call("mpsb_ground_state_search", At.ctx.h, At.h, H.h, int(maxsweeps), float(converge_rat),
+              float(eigs_tol), C.byref(ae))
+    return ae.value
+
+
+def product_mpo(O2, O1, ctx=None):
+    """The MPO of O2 * O1 (O1 applied first), fused bond index w1 + W1 * w2: the operator that
+    A_prod_L_OO_R_eigs (src/MatrixProductStates.jl:260-266) applies with O1 = L, O2 = Lconj."""
+    sites = []
+    for k in range(O1.na):
+        a, b = O1.site(k), O2.site(k)   # [w, d_out, w', d_in]
+        p = np.einsum("atbs,cudt->acubds", a, b)
+        w1, w2, dd, w1p, w2p = a.shape[0], b.shape[0], b.shape[1], a.shape[2], b.shape[2]
+        sites.append(p.reshape((w1 * w2, dd, w1p * w2p, a.shape[3]), order="F"))
+    return MPO.from_sites(sites, ctx or O1.ctx)
+
+
+def steady_state_search_(At, L, Lconj, maxsweeps, converge_rat, eigs_tol):
+    """src/steadystate.jl:6-86: ground_state_search! with the effective operator Lconj * L
+    (A_prod_L_OO_R_eigs with 4-index environments is the same contraction with the two MPO
+    bonds fused)."""
+    return ground_state_search_(At, product_mpo(Lconj, L, At.ctx), maxsweeps, converge_rat, eigs_tol)
+
+
 # ------------------------------------------------------------------ norms, gauge, observables
 
 def _scalar(name, *args):

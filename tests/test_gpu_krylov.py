@@ -84,3 +84,61 @@ def test_arnoldi_expm_matches_oracle(gpu_ctx, na, chi, numv):
     else:
         _sites_close(grhov[0], want, 1e-9)
     assert 1 - fidelity(got, want) < 1e-12
+
+
+def _tfi_mpo(na, J=1.0, h=0.7):
+    I, Z, X = np.eye(2), np.diag([1.0, -1.0]), np.array([[0.0, 1.0], [1.0, 0.0]])
+    W = np.zeros((3, 2, 3, 2), dtype=np.complex128)
+    W[0, :, 0, :] = I
+    W[1, :, 0, :] = Z
+    W[2, :, 0, :] = -h * X
+    W[2, :, 1, :] = -J * Z
+    W[2, :, 2, :] = I
+    return [W[2:3].copy()] + [W.copy() for _ in range(na - 2)] + [W[:, :, 0:1].copy()]
+
+
+def _real_lo_guess(na, chi, seed):
+    rng = np.random.default_rng(seed)
+    A, dims = R.mpsrandom(na, chi, 2, rng)
+    A = [a.real.astype(np.complex128) for a in A]
+    R.leftorthonormalizationQR_(A)
+    return A, dims
+
+
+@pytest.mark.parametrize("na,chi,sweeps", [(8, 16, 3), (12, 8, 2)])
+def test_ground_state_search_matches_oracle(gpu_ctx, na, chi, sweeps):
+    """ground_state_search! (src/groundstate.jl:67-147): eigenvalue and state (full and truncated
+    bond dimension); at full bond dimension also the exact ground energy."""
+    import mpsb200 as K
+    from oracle import groundstate as G
+    H = _tfi_mpo(na)
+    A, _ = _real_lo_guess(na, chi, 2)
+    gA = K.MPS.from_sites(A, gpu_ctx)
+    ae_ref = G.ground_state_search_(A, H, sweeps, 10.0, 1e-12)
+    ae = K.ground_state_search_(gA, K.MPO.from_sites(H, gpu_ctx), sweeps, 10.0, 1e-12)
+    assert abs(ae - ae_ref) < 1e-10 * abs(ae_ref)
+    assert 1 - fidelity(gA.sites(), A) < 1e-10
+    if chi >= 2 ** (na // 2):
+        assert abs(ae - np.linalg.eigvalsh(D.mpo_to_dense(H))[0]) < 1e-10 * abs(ae)
+
+
+def test_steady_state_search_matches_oracle(gpu_ctx):
+    """steady_state_search! (src/steadystate.jl:6-86) for a real non-Hermitian L: the lowest
+    eigenvalue of L^dagger L (zero at a steady state) and its state."""
+    import mpsb200 as K
+    from oracle import groundstate as G
+    na = 6
+    L = _tfi_mpo(na, J=1.0, h=0.4)
+    for o in L:                              # a longitudinal field: non-degenerate lowest level
+        o[o.shape[0] - 1, :, 0, :] += -0.3 * np.diag([1.0, -1.0])
+    for o in L[1:-1]:                        # non-Hermitian: an asymmetric hopping term
+        o[1, :, 0, :] = np.array([[0.0, 1.3], [0.2, 0.0]])
+    Lconj = [np.conj(o.transpose(0, 3, 2, 1)) for o in L]
+    A, _ = _real_lo_guess(na, 8, 3)
+    gA = K.MPS.from_sites(A, gpu_ctx)
+    ae_ref = G.steady_state_search_(A, L, Lconj, 3, 10.0, 1e-12)
+    ae = K.steady_state_search_(gA, K.MPO.from_sites(L, gpu_ctx), K.MPO.from_sites(Lconj, gpu_ctx), 3, 10.0, 1e-12)
+    Ld = D.mpo_to_dense(L)
+    assert abs(ae - ae_ref) < 1e-10 * max(1.0, abs(ae_ref))
+    assert abs(ae - np.linalg.eigvalsh(Ld.conj().T @ Ld)[0]) < 1e-9 * max(1.0, abs(ae))
+    assert 1 - fidelity(gA.sites(), A) < 1e-10
