@@ -208,6 +208,12 @@ int mpsb_op_update_le(mpsb_ctx* ctx, const void* A0, const void* AOL, void* env,
  * on the GPU (other streams, other host threads) race; serialise them on one stream. */
 int mpsb_op_prod_AOR_noalloc(void* stream, const void* A, const void* O, const void* R, void* AOR,
                              int chiL, int d, int chiR, int wL, int wR, int chiR0);
+/* svd(M) as compressionSVD! calls it (src/compression.jl:1296): thin SVD X = U diag(S) V^H of a
+ * device m x n column-major matrix, k = min(m, n); U (m x k) and V (n x k) device, S (k) host,
+ * singular values descending.  One-sided Jacobi (relative accuracy); phases of the singular
+ * vectors are those of the rotation sequence (LAPACK's are equally arbitrary). */
+int mpsb_op_svd(mpsb_ctx* ctx, const void* X, void* U, double* S, void* V, int m, int n);
+
 /* Q of the LAPACK geqrf+orgqr QR of the column-major m x n matrix X (m >= n):
  * qrq!(X)  src/orthonormalisation.jl:180-184. Q may alias X. R (n x n) optional (NULL). */
 int mpsb_op_qr(mpsb_ctx* ctx, const void* X, void* Q, void* R, int m, int n);

@@ -146,6 +146,7 @@ int mpsb_ctx_destroy(mpsb_ctx* ctx) {
     if (b.p) cudaFree(b.p);
   if (ctx->ws.splitk.p) cudaFree(ctx->ws.splitk.p);
   if (ctx->ws.qr.p) cudaFree(ctx->ws.qr.p);
+  if (ctx->ws.svd.p) cudaFree(ctx->ws.svd.p);
   cudaFree(ctx->d_scalars);
   cudaFreeHost(ctx->h_scalars);
   cudaStreamDestroy(ctx->own_stream);
@@ -627,6 +628,16 @@ int mpsb_op_update_le(mpsb_ctx* ctx, const void* A0, const void* AOL, void* env,
                       int chiR0) {
   MPSB_TRY(bind(ctx));
   return op_update_le(ctx, DP(A0), DP(AOL), DW(env), chiL0, d, chiR, wR, chiR0);
+}
+
+int mpsb_op_svd(mpsb_ctx* ctx, const void* X, void* U, double* S, void* V, int m, int n) {
+  MPSB_TRY(bind(ctx));
+  if (!X || !U || !S || !V || m < 1 || n < 1) return MPSB_ERR_DIMENSION;
+  void* before = ctx->ws.svd.p;
+  int st = svd_launch(m, n, DP(X), 1, m, DW(U), 1, m, S, DW(V), 1, n, &ctx->ws, ctx->stream);
+  if (ctx->ws.svd.p != before) ctx->ws_generation++;
+  MPSB_TRY(st);
+  return sync(ctx);
 }
 
 int mpsb_op_qr(mpsb_ctx* ctx, const void* X, void* Q, void* R, int m, int n) {

@@ -103,5 +103,8 @@ struct Workspace;
 // Q (and R) of each problem; uses the workspace's QR scratch (V, tau, V^H V, T V1^H)
 int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s);
 bool qr_supported(int m, int n);
+// thin SVD X = U diag(S) V^H by one-sided Jacobi (S on the host, descending)
+int svd_launch(int m, int n, const cd* X, int64_t x_r, int64_t x_c, cd* U, int64_t u_r, int64_t u_c, double* S,
+               cd* V, int64_t v_r, int64_t v_c, Workspace* ws, cudaStream_t st);
 
 }  // namespace mpsb

@@ -1,0 +1,205 @@
+// Thin SVD of a complex m x n matrix (FP64) by one-sided (Hestenes) Jacobi, for the truncation
+// rule of compressionSVD! (src/compression.jl:1280-1312), whose `svd` is LAPACK's.
+//
+// The columns of W = X (or X^H when m < n, then U and V swap roles) are rotated pairwise until
+// mutually orthogonal; V accumulates the rotations, the singular values are the final column
+// norms, U the normalised columns.  For a pair (p, q) with alpha = |w_p|^2, beta = |w_q|^2,
+// gamma = w_p^H w_q = |gamma| e^{i phi}: with b = e^{-i phi} w_q the 2x2 Gram matrix is real,
+// zeta = (beta - alpha) / (2 |gamma|), t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)),
+// c = 1 / sqrt(1 + t^2), s = c t, and w_p <- c w_p - s b, w_q <- s w_p + c b (likewise V).
+// Relative accuracy of one-sided Jacobi holds for the small singular values as well, which the
+// cumulative-weight cut of the truncation rule relies on.
+//
+// B200 mapping: one cooperative launch per matrix; CTA b takes pair b of each round of the
+// round-robin tournament (n_pad / 2 disjoint pairs per round, n_pad - 1 rounds per sweep),
+// reduces the three inner products over the rows with warp shuffles, rotates its two columns
+// of W and V, and the grid barrier separates rounds.  A sweep in which no pair needed a
+// rotation ends the loop; at most SVD_MAX_SWEEPS sweeps run (the kernel always finishes).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+#include "workspace.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace mpsb {
+namespace {
+
+constexpr int SVD_NT = 256, SVD_MAX_SWEEPS = 60;
+
+__device__ __forceinline__ cd block_sum(cd v, cd* red) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  cd s = cmk(0.0, 0.0);
+  for (int w = 0; w < SVD_NT / 32; ++w) s = cadd(s, red[w]);   // fixed order: reproducible
+  return s;
+}
+
+// partner of slot i in round r of the circle method over np (even) players: player 0 fixed
+__device__ __forceinline__ void round_pair(int r, int b, int np, int& p, int& q) {
+  const int m = np - 1;
+  auto pos = [&](int slot) { return slot == 0 ? 0 : 1 + (slot - 1 + r) % m; };
+  p = pos(b);
+  q = pos(np - 1 - b);
+  if (p > q) { const int t = p; p = q; q = t; }
+}
+
+__global__ void __launch_bounds__(SVD_NT) jacobi_kernel(int m, int np, cd* W, cd* V, int* flags, double eps) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ cd red[SVD_NT / 32];
+  __shared__ int s_rot;
+  const int b = blockIdx.x;
+  for (int sweep = 0; sweep < SVD_MAX_SWEEPS; ++sweep) {
+    for (int r = 0; r < np - 1; ++r) {
+      int p, q;
+      round_pair(r, b, np, p, q);
+      cd* wp = W + (int64_t)p * m;
+      cd* wq = W + (int64_t)q * m;
+      cd a = cmk(0.0, 0.0), g = cmk(0.0, 0.0);
+      double bb = 0.0;
+      for (int i = threadIdx.x; i < m; i += SVD_NT) {
+        const cd x = wp[i], y = wq[i];
+        a.x += x.x * x.x + x.y * x.y;
+        bb += y.x * y.x + y.y * y.y;
+        cfma_cj(g, x, y);
+      }
+      a.y = bb;
+      const cd ab = block_sum(a, red);
+      const cd gm = block_sum(g, red);
+      const double alpha = ab.x, beta = ab.y, ag = sqrt(gm.x * gm.x + gm.y * gm.y);
+      if (ag > eps * sqrt(alpha * beta) && ag > 0.0) {
+        const double zeta = (beta - alpha) / (2.0 * ag);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        const cd ph = cmk(gm.x / ag, -gm.y / ag);   // e^{-i phi}
+        for (int i = threadIdx.x; i < m; i += SVD_NT) {
+          const cd x = wp[i], y = cmul(ph, wq[i]);
+          wp[i] = cmk(c * x.x - s * y.x, c * x.y - s * y.y);
+          wq[i] = cmk(s * x.x + c * y.x, s * x.y + c * y.y);
+        }
+        cd* vp = V + (int64_t)p * np;
+        cd* vq = V + (int64_t)q * np;
+        for (int i = threadIdx.x; i < np; i += SVD_NT) {
+          const cd x = vp[i], y = cmul(ph, vq[i]);
+          vp[i] = cmk(c * x.x - s * y.x, c * x.y - s * y.y);
+          vq[i] = cmk(s * x.x + c * y.x, s * x.y + c * y.y);
+        }
+        if (threadIdx.x == 0) atomicOr(&flags[sweep], 1);
+      }
+      grid.sync();
+    }
+    if (threadIdx.x == 0) s_rot = atomicAdd(&flags[sweep], 0);
+    __syncthreads();
+    if (s_rot == 0) break;   // every CTA reads the same final flag of this sweep
+    grid.sync();
+  }
+}
+
+// W <- op(X) (X^H when `adj`), padded with a zero column to even width; V <- I
+__global__ void svd_init_kernel(int m, int n, int np, const cd* X, int64_t xr, int64_t xc, bool adj, cd* W, cd* V) {
+  const int64_t tw = (int64_t)m * np, tv = (int64_t)np * np;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tw + tv; e += (int64_t)gridDim.x * blockDim.x) {
+    if (e < tw) {
+      const int i = (int)(e % m), j = (int)(e / m);
+      cd v = cmk(0.0, 0.0);
+      if (j < n) v = adj ? cconj(X[(int64_t)j * xr + (int64_t)i * xc]) : X[(int64_t)i * xr + (int64_t)j * xc];
+      W[e] = v;
+    } else {
+      const int64_t f = e - tw;
+      V[f] = cmk((f % np) == (f / np) ? 1.0 : 0.0, 0.0);
+    }
+  }
+}
+
+__global__ void col_norms_kernel(int m, int np, const cd* W, double* s) {
+  __shared__ cd red[SVD_NT / 32];
+  const cd* w = W + (int64_t)blockIdx.x * m;
+  cd a = cmk(0.0, 0.0);
+  for (int i = threadIdx.x; i < m; i += SVD_NT) a.x += w[i].x * w[i].x + w[i].y * w[i].y;
+  a = block_sum(a, red);
+  if (threadIdx.x == 0) s[blockIdx.x] = sqrt(a.x);
+}
+
+// sorted outputs: Lout[:, k] = W[:, perm[k]] / s (left vectors of op(X)), Rout[:, k] = V[:, perm[k]]
+__global__ void svd_gather_kernel(int m, int np, int k, const cd* W, const cd* V, const double* s, const int* perm,
+                                  cd* Lout, int64_t l_r, int64_t l_c, cd* Rout, int64_t r_r, int64_t r_c, int nr) {
+  const int64_t tl = (int64_t)m * k, tr = (int64_t)nr * k;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tl + tr; e += (int64_t)gridDim.x * blockDim.x) {
+    if (e < tl) {
+      const int i = (int)(e % m), j = (int)(e / m), c = perm[j];
+      const double sv = s[c];
+      const cd w = W[(int64_t)c * m + i];
+      Lout[i * l_r + (int64_t)j * l_c] = sv > 0 ? cmk(w.x / sv, w.y / sv) : cmk(0.0, 0.0);
+    } else {
+      const int64_t f = e - tl;
+      const int i = (int)(f % nr), j = (int)(f / nr);
+      Rout[i * r_r + (int64_t)j * r_c] = V[(int64_t)perm[j] * np + i];
+    }
+  }
+}
+
+}  // namespace
+
+// Thin SVD X = U diag(S) V^H (m x n, k = min(m, n) singular values, descending, S on the host
+// and in `dS` if non-null).  U: m x k with strides (u_r, u_c); V: n x k with (v_r, v_c).
+int svd_launch(int m, int n, const cd* X, int64_t x_r, int64_t x_c, cd* U, int64_t u_r, int64_t u_c, double* S,
+               cd* V, int64_t v_r, int64_t v_c, Workspace* ws, cudaStream_t st) {
+  if (m < 1 || n < 1) return MPSB_ERR_DIMENSION;
+  const bool adj = m < n;
+  const int mm = adj ? n : m, nn = adj ? m : n, np = nn + (nn & 1), k = nn;
+  if (np / 2 > 1024) return MPSB_ERR_UNSUPPORTED;
+  const size_t bytes = ((size_t)mm * np + (size_t)np * np) * sizeof(cd) + np * sizeof(double) + np * sizeof(int) +
+                       SVD_MAX_SWEEPS * sizeof(int) + 64;
+  MPSB_TRY(devbuf_ensure(ws, ws->svd, bytes));
+  cd* W = static_cast<cd*>(ws->svd.p);
+  cd* Vw = W + (int64_t)mm * np;
+  double* dS = reinterpret_cast<double*>(Vw + (int64_t)np * np);
+  int* dperm = reinterpret_cast<int*>(dS + np);
+  int* flags = dperm + np;
+  MPSB_CUDA_TRY(cudaMemsetAsync(flags, 0, SVD_MAX_SWEEPS * sizeof(int), st));
+  count_launch(ws);
+  svd_init_kernel<<<148 * 4, 256, 0, st>>>(mm, nn, np, X, x_r, x_c, adj, W, Vw);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  if (np >= 2) {
+    int nb = np / 2;
+    int mmv = mm;
+    double eps = 1e-15;
+    void* args[] = {&mmv, (void*)&np, &W, &Vw, &flags, &eps};
+    count_launch(ws);
+    MPSB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)jacobi_kernel, dim3(nb), dim3(SVD_NT), args, 0, st));
+  }
+  count_launch(ws);
+  col_norms_kernel<<<np, SVD_NT, 0, st>>>(mm, np, W, dS);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  std::vector<double> hs(np);
+  MPSB_CUDA_TRY(cudaMemcpyAsync(hs.data(), dS, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+  MPSB_CUDA_TRY(cudaStreamSynchronize(st));
+  std::vector<int> perm(np);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.begin() + np, [&](int a, int b) { return hs[a] > hs[b]; });
+  // the padding column (zero) sorts last; keep the k largest
+  for (int j = 0; j < k; ++j) S[j] = hs[perm[j]];
+  MPSB_CUDA_TRY(cudaMemcpyAsync(dperm, perm.data(), np * sizeof(int), cudaMemcpyHostToDevice, st));
+  count_launch(ws);
+  // op(X) = L S R^H with L = normalised W, R = V: for X itself U = L, V = R; for X^H, U = R, V = L
+  if (!adj)
+    svd_gather_kernel<<<148 * 4, 256, 0, st>>>(mm, np, k, W, Vw, dS, dperm, U, u_r, u_c, V, v_r, v_c, nn);
+  else
+    svd_gather_kernel<<<148 * 4, 256, 0, st>>>(mm, np, k, W, Vw, dS, dperm, V, v_r, v_c, U, u_r, u_c, nn);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  return MPSB_OK;
+}
+
+}  // namespace mpsb

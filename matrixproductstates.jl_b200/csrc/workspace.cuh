@@ -13,6 +13,7 @@ struct DevBuf {
 struct Workspace {
   DevBuf splitk;          // split-K partial tiles
   DevBuf qr;              // QR: reflectors, tau, V^H V and T V1^H
+  DevBuf svd;             // SVD: the Jacobi working matrix, V, norms, flags
   DevBuf named[16];       // per-sweep temporaries (see engine.cu)
   bool capturing = false;
   int64_t launches = 0;   // kernel launches issued (eager) or recorded (capture)

@@ -96,6 +96,41 @@ def test_qr_blocked_rank_deficient_padded_site(gpu_ctx):
     assert np.abs(Q - q_ref).max() < 1e-12
 
 
+@pytest.mark.parametrize("m,n", [(1, 1), (1, 8), (8, 1), (64, 16), (16, 64), (128, 128), (512, 131), (96, 600)])
+def test_svd_matches_lapack(gpu_ctx, m, n):
+    """Thin SVD (the `svd` of compressionSVD!): singular values to relative accuracy, the
+    factors orthonormal and reproducing X (vectors are unique only up to phases)."""
+    rng = np.random.default_rng(m * 7 + n)
+    X = crand(rng, m, n)
+    X[:, :: max(1, n // 5)] *= 1e-6                      # a spread of singular values
+    k = min(m, n)
+    s_ref = np.linalg.svd(X, compute_uv=False)
+    dX, dU, dV = to_dev(X), empty_dev((m, k)), empty_dev((n, k))
+    S = np.zeros(k)
+    _call(gpu_ctx, "mpsb_op_svd", _p(dX), _p(dU), S.ctypes.data_as(C.POINTER(C.c_double)), _p(dV), m, n)
+    U, V = from_dev(dU, (m, k)), from_dev(dV, (n, k))
+    assert np.all(np.diff(S) <= 0)
+    assert np.abs(S - s_ref).max() <= 1e-12 * s_ref[0]
+    big = s_ref > 1e-9 * s_ref[0]
+    assert np.abs(S[big] / s_ref[big] - 1).max() < 1e-9
+    assert np.abs((U * S) @ V.conj().T - X).max() < 1e-12 * s_ref[0]
+    assert np.abs(U.conj().T @ U - np.eye(k)).max() < 1e-12
+    assert np.abs(V.conj().T @ V - np.eye(k)).max() < 1e-12
+
+
+def test_svd_rank_deficient(gpu_ctx):
+    rng = np.random.default_rng(5)
+    X = crand(rng, 40, 6) @ crand(rng, 6, 30)            # rank 6
+    X[:, 3] = 0
+    S = np.zeros(30)
+    dX, dU, dV = to_dev(X), empty_dev((40, 30)), empty_dev((30, 30))
+    _call(gpu_ctx, "mpsb_op_svd", _p(dX), _p(dU), S.ctypes.data_as(C.POINTER(C.c_double)), _p(dV), 40, 30)
+    U, V = from_dev(dU, (40, 30)), from_dev(dV, (30, 30))
+    s_ref = np.linalg.svd(X, compute_uv=False)
+    assert np.abs(S - s_ref).max() < 1e-12 * s_ref[0]
+    assert np.abs((U[:, :6] * S[:6]) @ V[:, :6].conj().T - X).max() < 1e-12 * s_ref[0]
+
+
 SHAPES = [  # chiL, d, chiR, wL, wR, chi0
     (1, 2, 2, 1, 4, 2), (4, 2, 8, 4, 4, 8), (32, 2, 32, 4, 4, 32), (17, 3, 29, 5, 3, 23),
     (128, 4, 128, 8, 8, 128), (64, 4, 128, 6, 6, 100),
