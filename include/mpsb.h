@@ -208,6 +208,14 @@ int mpsb_op_update_le(mpsb_ctx* ctx, const void* A0, const void* AOL, void* env,
  * on the GPU (other streams, other host threads) race; serialise them on one stream. */
 int mpsb_op_prod_AOR_noalloc(void* stream, const void* A, const void* O, const void* R, void* AOR,
                              int chiL, int d, int chiR, int wL, int wR, int chiR0);
+/* compressionSVD!(mps, dmax, tol)  src/compression.jl:1280-1312 -- the truncation rule
+ * chi_new = min(#{cumsum(s^2/sum s^2) < 1 - tol} + 1, dmax) applied site by site from the right
+ * to a left-canonical MPS.  The reference resizes mps in place; here the result (right
+ * canonical, new bond dims) is a new handle *out.  err_trim and ent_ent (na values, host) and
+ * *err_glob are the reference's return values. */
+int mpsb_compression_svd(mpsb_ctx* ctx, const mpsb_mps* in, int dmax, double tol, mpsb_mps** out,
+                         double* err_glob, double* err_trim, double* ent_ent);
+
 /* svd(M) as compressionSVD! calls it (src/compression.jl:1296): thin SVD X = U diag(S) V^H of a
  * device m x n column-major matrix, k = min(m, n); U (m x k) and V (n x k) device, S (k) host,
  * singular values descending.  One-sided Jacobi (relative accuracy); phases of the singular

@@ -630,6 +630,22 @@ int mpsb_op_update_le(mpsb_ctx* ctx, const void* A0, const void* AOL, void* env,
   return op_update_le(ctx, DP(A0), DP(AOL), DW(env), chiL0, d, chiR, wR, chiR0);
 }
 
+int mpsb_compression_svd(mpsb_ctx* ctx, const mpsb_mps* in, int dmax, double tol, mpsb_mps** out, double* err_glob,
+                         double* err_trim, double* ent_ent) {
+  MPSB_TRY(bind(ctx));
+  if (!in || !out) return MPSB_ERR_INVALID_ARG;
+  std::vector<int64_t> dims;
+  cd* sites = nullptr;
+  MPSB_TRY(compression_svd(ctx, in, dmax, tol, dims, &sites, err_glob, err_trim, ent_ent));
+  mpsb_mps* A = nullptr;
+  MPSB_TRY(mpsb_mps_create(ctx, in->na, in->d, dims.data(), &A));
+  for (int k = 0; k < in->na; ++k)
+    MPSB_CUDA_TRY(cudaMemcpyAsync(A->site(k), sites + in->off[k], A->site_elems(k) * sizeof(cd),
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+  *out = A;
+  return sync(ctx);
+}
+
 int mpsb_op_svd(mpsb_ctx* ctx, const void* X, void* U, double* S, void* V, int m, int n) {
   MPSB_TRY(bind(ctx));
   if (!X || !U || !S || !V || m < 1 || n < 1) return MPSB_ERR_DIMENSION;

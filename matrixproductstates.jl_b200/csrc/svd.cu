@@ -203,3 +203,118 @@ int svd_launch(int m, int n, const cd* X, int64_t x_r, int64_t x_c, cd* U, int64
 }
 
 }  // namespace mpsb
+
+// ---- compressionSVD! (src/compression.jl:1280-1312) -------------------------------------
+#include "engine.cuh"
+
+namespace mpsb {
+namespace {
+
+// out (rows x cols, ld rows) = the conjugate transpose of the first `rows` columns of V (cols x rows used)
+__global__ void adjoint_cols_kernel(int rows, int cols, const cd* V, int64_t ldv, cd* out) {
+  const int64_t total = (int64_t)rows * cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e % rows), c = (int)(e / rows);
+    out[e] = cconj(V[(int64_t)r * ldv + c]);
+  }
+}
+// out[:, j] = U[:, j] * s[j], j < cols
+__global__ void scale_cols_kernel(int rows, int cols, const cd* U, const double* s, cd* out) {
+  const int64_t total = (int64_t)rows * cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e / rows);
+    out[e] = cmk(U[e].x * s[c], U[e].y * s[c]);
+  }
+}
+
+}  // namespace
+
+// Right-to-left truncating SVD sweep of a left-canonical MPS: at site i (dl, d, dr) with the
+// carried factor r (dr x b), M = reshape(A_i, dl d, dr) r, svd(reshape(M, dl, d b)) = u s v',
+// s <- s[s > 0], dnew = min(#{cumsum(s^2 / sum s^2) < 1 - tol} + 1, dmax), err_trim_i = the
+// dropped weight, ent_i = -2 sum s^2 log s, new A_i = reshape(v[:, 1:dnew]', dnew, d, b),
+// r = u[:, 1:dnew] diag(s[1:dnew]).  err_glob = 1 - |r|^2 at the end.  The new sites land in
+// context scratch at the old sites' offsets (no site grows); dims_out are the new bonds.
+int compression_svd(mpsb_ctx* ctx, const mpsb_mps* in, int dmax, double tol, std::vector<int64_t>& dims_out,
+                    cd** sites, double* err_glob, double* err_trim, double* ent_ent) {
+  if (!ctx || !in || dmax < 1 || !(tol >= 0)) return MPSB_ERR_INVALID_ARG;
+  const int na = in->na, d = in->d;
+  cudaStream_t st = ctx->stream;
+  int64_t maxsite = 1, maxr = 1;
+  for (int k = 0; k < na; ++k) {
+    maxsite = std::max<int64_t>(maxsite, in->site_elems(k));
+    maxr = std::max<int64_t>(maxr, in->dims[k] * in->dims[k]);
+  }
+  // scratch: new sites (old total), r, M, U, V, dS
+  cd* base = nullptr;
+  const size_t need = (size_t)in->total + 2 * maxr + 3 * maxsite + maxsite / 2 + 64;
+  MPSB_TRY(ensure_slot(ctx, SLOT_MISC, need * sizeof(cd), &base));
+  cd* out = base;
+  cd* r = out + in->total;
+  cd* r2 = r + maxr;
+  cd* M = r2 + maxr;
+  cd* U = M + maxsite;
+  cd* V = U + maxsite;
+  double* dS = reinterpret_cast<double*>(V + maxsite);
+  dims_out.assign(na + 1, 1);
+  MPSB_TRY(set_boundary(ctx, r, cmk(1.0, 0.0)));
+  int b = 1;   // current right bond (after truncation)
+  std::vector<double> S;
+  for (int i = na - 1; i >= 0; --i) {
+    const int dl = (int)in->dims[i], dr = (int)in->dims[i + 1];
+    {  // M (dl d x b) = A_i (dl d x dr) r (dr x b)
+      Gemm g;
+      g.M = dl * d; g.N = b; g.K = dr;
+      g.A = in->site(i); g.a_m = 1; g.a_k = (int64_t)dl * d;
+      g.B = r; g.b_k = 1; g.b_n = dr;
+      g.C = M; g.c_m = 1; g.c_n = (int64_t)dl * d;
+      MPSB_TRY(run_gemm(ctx, g));
+    }
+    const int mm = dl, nn = d * b, k = std::min(mm, nn);
+    S.assign(k, 0.0);
+    MPSB_TRY(svd_launch(mm, nn, M, 1, mm, U, 1, mm, S.data(), V, 1, nn, &ctx->ws, st));
+    int kp = 0;
+    double stot = 0.0, ent = 0.0;
+    while (kp < k && S[kp] > 0) {
+      stot += S[kp] * S[kp];
+      ent += S[kp] * S[kp] * std::log(S[kp]);
+      ++kp;
+    }
+    if (kp == 0) {
+      set_last_message("compressionSVD: site %d is zero", i + 1);
+      return MPSB_ERR_NONFINITE;
+    }
+    int below = 0;
+    double cum = 0.0;
+    for (int j = 0; j < kp; ++j) {
+      cum += S[j] * S[j] / stot;
+      if (cum < 1.0 - tol) ++below;
+    }
+    // below + 1 can exceed the number of positive singular values when tol is below the rounding
+    // of the cumulative sum (the reference then fails on v[:, 1:dnew]); keep them all instead
+    const int dnew = std::min(std::min(below + 1, dmax), kp);
+    double dropped = 0.0;
+    for (int j = dnew; j < kp; ++j) dropped += S[j] * S[j];
+    if (err_trim) err_trim[i] = dropped / stot;
+    if (ent_ent) ent_ent[i] = -2.0 * ent;
+    // new site i = v[:, 1:dnew]' as (dnew, d, b); r = u[:, 1:dnew] diag(s)
+    count_launch(&ctx->ws);
+    adjoint_cols_kernel<<<148 * 2, 256, 0, st>>>(dnew, nn, V, nn, out + in->off[i]);
+    MPSB_CUDA_TRY(cudaGetLastError());
+    MPSB_CUDA_TRY(cudaMemcpyAsync(dS, S.data(), dnew * sizeof(double), cudaMemcpyHostToDevice, st));
+    count_launch(&ctx->ws);
+    scale_cols_kernel<<<148 * 2, 256, 0, st>>>(mm, dnew, U, dS, r2);
+    MPSB_CUDA_TRY(cudaGetLastError());
+    std::swap(r, r2);
+    dims_out[i] = dnew;
+    b = dnew;
+  }
+  cd r0;
+  MPSB_CUDA_TRY(cudaMemcpyAsync(&r0, r, sizeof(cd), cudaMemcpyDeviceToHost, st));
+  MPSB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (err_glob) *err_glob = 1.0 - (r0.x * r0.x + r0.y * r0.y);
+  *sites = out;
+  return MPSB_OK;
+}
+
+}  // namespace mpsb

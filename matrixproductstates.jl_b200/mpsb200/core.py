@@ -463,6 +463,25 @@ def steady_state_search_(At, L, Lconj, maxsweeps, converge_rat, eigs_tol):
     return ground_state_search_(At, product_mpo(Lconj, L, At.ctx), maxsweeps, converge_rat, eigs_tol)
 
 
+def compressionSVD_(mps, dmax, tol=1e-15):
+    """src/compression.jl:1280-1312: right-to-left SVD truncation of the left-canonical mps to
+    bond dims <= dmax with relative weight tolerance tol.  The reference resizes mps in place;
+    a handle cannot change its dims, so the truncated (right-canonical) MPS is returned first:
+    (new_mps, err_glob, err_trim, ent_ent)."""
+    out = C.c_void_p()
+    eg = C.c_double()
+    et = np.zeros(mps.na)
+    ee = np.zeros(mps.na)
+    _lib.call("mpsb_compression_svd", mps.ctx.h, mps.h, int(dmax), float(tol), C.byref(out), C.byref(eg),
+              _dptr(et), _dptr(ee))
+    new = MPS.__new__(MPS)
+    new.ctx, new.na, new.d, new.h = mps.ctx, mps.na, mps.d, out
+    info = np.zeros(mps.na + 1, dtype=np.int64)
+    _lib.call("mpsb_mps_info", out, None, None, info.ctypes.data_as(C.POINTER(C.c_int64)))
+    new.dims = [int(x) for x in info]
+    return new, eg.value, et, ee
+
+
 # ------------------------------------------------------------------ norms, gauge, observables
 
 def _scalar(name, *args):

@@ -731,5 +731,30 @@ def RK4stp_apply_H_half_(dt, H, psi0, psi, psi1, psi2, psi3, env1, env2, env3, e
                                     [list(psi), psi1, psi2, psi3], H[2])
 
 
+def compressionSVD_(mps, dmax, tol=1e-15):
+    """src/compression.jl:1280-1312: right-to-left SVD truncation of a left-canonical MPS
+    (mps replaced site by site, bonds shrink); returns (err_glob, err_trim, ent_ent)."""
+    n = len(mps)
+    err_trim = np.zeros(n)
+    ent_ent = np.zeros(n)
+    dnew = 1
+    r = np.ones((1, 1), dtype=CT)
+    for i in range(n - 1, -1, -1):
+        dl, d, dr = mps[i].shape
+        mps_site = jr(mps[i], dl * d, dr) @ r
+        u, s, vh = np.linalg.svd(jr(mps_site, dl, dnew * d), full_matrices=False)
+        s = s[s > 0]
+        stot = np.sum(s ** 2)
+        b = dnew
+        dnew = min(int(np.sum(np.cumsum(s ** 2 / stot) < (1 - tol))) + 1, dmax)
+        err_trim[i] = np.sum(s[dnew:] ** 2) / stot
+        ent_ent[i] = -2 * np.sum(s ** 2 * np.log(s))
+        v = vh.conj().T
+        mps[i] = jr(v[:, :dnew].conj().T, dnew, d, b)
+        r = u[:, :dnew] @ np.diag(s[:dnew])
+    err_glob = 1 - abs(r[0, 0]) ** 2
+    return err_glob, err_trim, ent_ent
+
+
 def copy_mps(mps):
     return [np.array(a, dtype=CT, copy=True) for a in mps]

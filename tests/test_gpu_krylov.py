@@ -142,3 +142,21 @@ def test_steady_state_search_matches_oracle(gpu_ctx):
     assert abs(ae - ae_ref) < 1e-10 * max(1.0, abs(ae_ref))
     assert abs(ae - np.linalg.eigvalsh(Ld.conj().T @ Ld)[0]) < 1e-9 * max(1.0, abs(ae))
     assert 1 - fidelity(gA.sites(), A) < 1e-10
+
+
+@pytest.mark.parametrize("dmax,tol", [(16, 1e-15), (6, 1e-4), (9, 1e-12)])
+def test_compression_svd_matches_oracle(gpu_ctx, dmax, tol):
+    """compressionSVD! (src/compression.jl:1280-1312): new bond dims, the errors and entropies,
+    and the truncated state (singular vectors are unique only up to phases)."""
+    import mpsb200 as K
+    rng = np.random.default_rng(40)
+    A, dims = R.mpsrandom(9, 16, 2, rng)
+    A[-1] = A[-1] * 0.9
+    B = R.copy_mps(A)
+    eg, et, ee = R.compressionSVD_(B, dmax, tol)
+    gnew, geg, get, gee = K.compressionSVD_(K.MPS.from_sites(A, gpu_ctx), dmax, tol)
+    assert gnew.dims == [1] + [b.shape[2] for b in B]
+    assert abs(geg - eg) < 1e-12
+    assert np.abs(get - et).max() < 1e-12
+    assert np.abs(gee - ee).max() < 1e-10
+    assert 1 - fidelity(gnew.sites(), B) < 1e-12

@@ -331,3 +331,26 @@ def test_ground_state_search_tfi_matches_exact_diagonalisation():
     psi = D.mps_to_dense(A)
     assert abs(ae - e0) < 1e-10 * abs(e0)
     assert abs((psi.conj() @ D.mpo_to_dense(H) @ psi).real / np.vdot(psi, psi).real - e0) < 1e-10 * abs(e0)
+
+
+def test_compression_svd_rule_and_exactness():
+    """compressionSVD! (src/compression.jl:1280-1312): untruncated it reproduces the state (right
+    canonical, err_glob = 1 - <psi|psi>); truncated, the dropped weights follow the rule."""
+    rng = np.random.default_rng(12)
+    A, dims = R.mpsrandom(8, 16, 2, rng)
+    A[-1] = A[-1] * 0.8
+    psi = D.mps_to_dense(A)
+    B = R.copy_mps(A)
+    eg, et, ee = R.compressionSVD_(B, 16, 1e-15)
+    assert [b.shape[2] for b in B[:-1]] == dims[1:-1]
+    assert abs(eg - (1 - 0.64)) < 1e-12 and np.abs(et).max() < 1e-14
+    for b in B[1:]:   # right canonical
+        m = b.reshape(b.shape[0], -1, order="F")
+        assert np.abs(m @ m.conj().T - np.eye(b.shape[0])).max() < 1e-12
+    got = D.mps_to_dense(B)
+    assert abs(abs(np.vdot(got, psi)) / (np.linalg.norm(got) * np.linalg.norm(psi)) - 1) < 1e-12
+    C = R.copy_mps(A)
+    eg2, et2, ee2 = R.compressionSVD_(C, 5, 1e-3)
+    assert max(c.shape[2] for c in C) <= 5
+    assert np.all(et2 >= 0) and et2.max() > 0
+    assert abs(ee2[-1] - ee[-1]) < 1e-12   # the first site processed sees the untruncated spectrum
