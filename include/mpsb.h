@@ -64,7 +64,9 @@ int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out);
 int mpsb_mps_create(mpsb_ctx* ctx, int na, int d, const int64_t* dims /* na+1 */, mpsb_mps** out);
 int mpsb_mps_destroy(mpsb_mps* A);
 int mpsb_mps_info(const mpsb_mps* A, int* na, int* d, int64_t* dims /* na+1, may be NULL */);
-/* site is 1-based like the reference; host buffer holds dims[site-1]*d*dims[site] complex */
+/* site is 1-based like the reference; host buffer holds dims[site-1]*d*dims[site] complex.
+ * set_site is ordered on the context stream and returns without waiting for it: a pageable
+ * host buffer may be reused on return, a pinned one only after mpsb_sync.  get_site waits. */
 int mpsb_mps_set_site(mpsb_mps* A, int site, const double* host);
 int mpsb_mps_get_site(const mpsb_mps* A, int site, double* host);
 /* device pointer of a site (for zero-copy interop); site 1-based */
@@ -75,6 +77,7 @@ int mpsb_mps_copy(mpsb_mps* dst, const mpsb_mps* src);
 /* ---------------------------------------------------------------- MPO (Vector{Array{T,4}}) */
 int mpsb_mpo_create(mpsb_ctx* ctx, int na, int d, const int64_t* w /* na+1 */, mpsb_mpo** out);
 int mpsb_mpo_destroy(mpsb_mpo* O);
+/* same stream ordering as mpsb_mps_set_site */
 int mpsb_mpo_set_site(mpsb_mpo* O, int site, const double* host);
 int mpsb_mpo_get_site(const mpsb_mpo* O, int site, double* host);
 

@@ -57,8 +57,17 @@ static int dev_alloc(cd** p, int64_t elems) {
   return MPSB_OK;
 }
 
+// Stream-ordered: later work on the context stream sees the data.  From pageable memory the
+// copy has left the host buffer when this returns; from pinned (page-locked) memory it has not,
+// and the buffer must stay unchanged until the stream passes the copy (mpsb_sync).
 static int upload(mpsb_ctx* ctx, cd* dst, const double* host, int64_t elems) {
   MPSB_CUDA_TRY(cudaMemcpyAsync(dst, host, (size_t)elems * sizeof(cd), cudaMemcpyHostToDevice, ctx->stream));
+  return MPSB_OK;
+}
+
+// the same, waiting for the copy (small operator buffers the caller may reuse at once)
+static int upload_wait(mpsb_ctx* ctx, cd* dst, const double* host, int64_t elems) {
+  MPSB_TRY(upload(ctx, dst, host, elems));
   return sync(ctx);
 }
 
@@ -483,7 +492,7 @@ int mpsb_apply_site_operator(mpsb_ctx* ctx, mpsb_mps* A, int site, const double*
   const int d = A->d, k = site - 1;
   cd* dop;
   MPSB_TRY(ensure_slot(ctx, SLOT_ENV1, (size_t)d * d * sizeof(cd), &dop));
-  MPSB_TRY(upload(ctx, dop, op, (int64_t)d * d));
+  MPSB_TRY(upload_wait(ctx, dop, op, (int64_t)d * d));
   MpoApply a;
   const int chiL = (int)A->dims[k], chiR = (int)A->dims[k + 1];
   a.X = chiL; a.Y = chiR; a.K1 = d; a.K2 = 1; a.M1 = d; a.M2 = 1;
@@ -549,7 +558,7 @@ int mpsb_measure_local(mpsb_ctx* ctx, const mpsb_mps* A, const double* op, doubl
   MPSB_TRY(ensure_slot(ctx, SLOT_MISC, maxS * sizeof(cd), &aenv));
   MPSB_TRY(ensure_slot(ctx, SLOT_T, (size_t)(d * d + na) * sizeof(cd), &dop));
   cd* res = dop + d * d;
-  MPSB_TRY(upload(ctx, dop, op, (int64_t)d * d));
+  MPSB_TRY(upload_wait(ctx, dop, op, (int64_t)d * d));
   count_launch(&ctx->ws);
   MPSB_TRY(set_value(e0, cmk(1.0, 0.0), ctx->stream));
   cd* cur = e0;
