@@ -57,6 +57,12 @@ int mpsb_sync(mpsb_ctx* ctx);
 int mpsb_ctx_set_stream(mpsb_ctx* ctx, void* stream);
 /* Capture each RK4 step into a CUDA graph and replay it (default on). */
 int mpsb_ctx_set_graphs(mpsb_ctx* ctx, int enable);
+/* Overlap, inside mpsb_rk4stp_apply_H_half, each stage's environment initialisation with the
+ * previous stage's sweep on a second stream (default on; MPSB_PIPELINE=0 in the environment
+ * turns it off at context creation).  Results are identical either way; with it on, the
+ * env1..env3 / envop buffers end up holding other stages' environments than the reference's
+ * (they are scratch to every reference caller).  No reference counterpart. */
+int mpsb_ctx_set_pipeline(mpsb_ctx* ctx, int enable);
 /* Kernel launches issued by this context since creation (for accounting). */
 int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out);
 

@@ -1,5 +1,6 @@
 // extern "C" entry points of include/mpsb.h.
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -132,6 +133,14 @@ int mpsb_ctx_create(int device, mpsb_ctx** out) {
   e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; set_last_error(e, "cudaStreamCreate", __FILE__, __LINE__); return MPSB_ERR_CUDA; }
   c->stream = c->own_stream;
+  e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(c->own_stream);
+    delete c;
+    set_last_error(e, "cudaStreamCreate", __FILE__, __LINE__);
+    return MPSB_ERR_CUDA;
+  }
+  if (const char* pe = getenv("MPSB_PIPELINE")) c->pipeline = atoi(pe) != 0;
   if (cudaMalloc((void**)&c->d_scalars, 64 * sizeof(double)) != cudaSuccess ||
       cudaMallocHost((void**)&c->h_scalars, 64 * sizeof(double)) != cudaSuccess) {
     cudaStreamDestroy(c->own_stream);
@@ -156,8 +165,14 @@ int mpsb_ctx_destroy(mpsb_ctx* ctx) {
   if (ctx->ws.splitk.p) cudaFree(ctx->ws.splitk.p);
   if (ctx->ws.qr.p) cudaFree(ctx->ws.qr.p);
   if (ctx->ws.svd.p) cudaFree(ctx->ws.svd.p);
+  cudaStreamSynchronize(ctx->side);
+  for (auto& b : ctx->ws_side.named)
+    if (b.p) cudaFree(b.p);
+  if (ctx->ws_side.splitk.p) cudaFree(ctx->ws_side.splitk.p);
+  for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
   cudaFree(ctx->d_scalars);
   cudaFreeHost(ctx->h_scalars);
+  cudaStreamDestroy(ctx->side);
   cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return MPSB_OK;
@@ -185,7 +200,13 @@ int mpsb_ctx_set_graphs(mpsb_ctx* ctx, int enable) {
 
 int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out) {
   if (!ctx || !out) return MPSB_ERR_INVALID_ARG;
-  *out = ctx->ws.launches;
+  *out = ctx->ws.launches + ctx->ws_side.launches;
+  return MPSB_OK;
+}
+
+int mpsb_ctx_set_pipeline(mpsb_ctx* ctx, int enable) {
+  if (!ctx) return MPSB_ERR_INVALID_ARG;
+  ctx->pipeline = enable != 0;
   return MPSB_OK;
 }
 

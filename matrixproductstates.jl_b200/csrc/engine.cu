@@ -228,13 +228,8 @@ static int sweep_scratch(mpsb_ctx* ctx, const mpsb_mps* A0, const mpsb_mpo* H, i
   return MPSB_OK;
 }
 
-// compress_sum_var_apply_H_left! (src/compression.jl:889-944) when !right,
-// compress_sum_var_apply_H_right! (src/compression.jl:1007-1063) when right.
-// numv == 1 with coef {1} is compress_var_apply_H_left! (src/compression.jl:321-347).
-int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* const* env, mpsb_env* envop,
-                             const mpsb_mps* Ain, const cd* coef, int numv, const mpsb_mps* const* A,
-                             const mpsb_mpo* H) {
-  if (!ctx || !A0 || !envop || !Ain || !coef || !A || !H || numv < 1) return MPSB_ERR_INVALID_ARG;
+static int sum_var_check(const mpsb_mps* A0, mpsb_env* const* env, const mpsb_env* envop, const mpsb_mps* Ain,
+                         int numv, const mpsb_mps* const* A, const mpsb_mpo* H) {
   const int np = numv - 1;
   if (!same_dims(A0, Ain)) return MPSB_ERR_DIMENSION;
   for (int l = 0; l < numv; ++l)
@@ -242,35 +237,74 @@ int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* 
   for (int l = 0; l < np; ++l)
     if (!env || !env[l] || env[l]->three || env[l]->na != A0->na) return MPSB_ERR_DIMENSION;
   if (!envop->three || envop->na != A0->na || H->na != A0->na || H->d != A0->d) return MPSB_ERR_DIMENSION;
-  const int na = A0->na, d = A0->d;
-  for (int k = 0; k <= na; ++k) {
+  for (int k = 0; k <= A0->na; ++k) {
     if (envop->d1[k] != A0->dims[k] || envop->d2[k] != A0->dims[k] || envop->w[k] != H->w[k]) return MPSB_ERR_DIMENSION;
     for (int l = 0; l < np; ++l)
       if (env[l]->d1[k] != A0->dims[k] || env[l]->d2[k] != A0->dims[k]) return MPSB_ERR_DIMENSION;
   }
-  SweepScratch s;
-  MPSB_TRY(sweep_scratch(ctx, A0, H, np, s));
-  const mpsb_mps* AH = A[np];
-  auto D = [&](int k) { return (int)A0->dims[k]; };
-  auto W = [&](int k) { return (int)H->w[k]; };
+  return MPSB_OK;
+}
 
+// Environment initialisation of a sum stage: left environments (L->R, for an R->L sweep) when
+// !right, right environments (R->L) when right, from the bra Ain and the terms A (the last one
+// through H), every chain advanced site by site in the order the previous stage finalises its
+// sites.  `wait`, when given, holds one event per site that is waited on before site k is read.
+static int sum_var_init(mpsb_ctx* ctx, bool right, mpsb_env* const* env, mpsb_env* envop, const mpsb_mps* Ain,
+                        const cd* coef, int numv, const mpsb_mps* const* A, const mpsb_mpo* H, const SweepScratch& s,
+                        const cudaEvent_t* wait) {
+  const int np = numv - 1, na = Ain->na, d = Ain->d;
+  const mpsb_mps* AH = A[np];
+  auto D = [&](int k) { return (int)Ain->dims[k]; };
+  auto W = [&](int k) { return (int)H->w[k]; };
   if (!right) {
-    // ---- left environments from Ain (bra) and the terms (kets)
     for (int l = 0; l < np; ++l) {
       MPSB_TRY(set_boundary(ctx, env[l]->entry(0), ONE));
-      for (int k = 0; k < na - 1; ++k) {
-        MPSB_TRY(op_L2_A3(ctx, env[l]->entry(k), A[l]->site(k), s.P[l], D(k), D(k), d * D(k + 1), ONE, ZERO, false));
-        MPSB_TRY(op_update_lenv(ctx, Ain->site(k), s.P[l], env[l]->entry(k + 1), D(k) * d, D(k + 1), D(k + 1), true));
-      }
       MPSB_TRY(set_boundary(ctx, env[l]->entry(na), coef[l]));
     }
     MPSB_TRY(set_boundary(ctx, envop->entry(0), ONE));
+    MPSB_TRY(set_boundary(ctx, envop->entry(na), coef[np]));
     for (int k = 0; k < na - 1; ++k) {
+      if (wait) MPSB_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, wait[k], 0));
+      for (int l = 0; l < np; ++l) {
+        MPSB_TRY(op_L2_A3(ctx, env[l]->entry(k), A[l]->site(k), s.P[l], D(k), D(k), d * D(k + 1), ONE, ZERO, false));
+        MPSB_TRY(op_update_lenv(ctx, Ain->site(k), s.P[l], env[l]->entry(k + 1), D(k) * d, D(k + 1), D(k + 1), true));
+      }
       MPSB_TRY(op_prod_AOL(ctx, AH->site(k), H->site(k), envop->entry(k), s.AOL, D(k), d, D(k + 1), W(k), W(k + 1), D(k)));
       MPSB_TRY(op_update_le(ctx, Ain->site(k), s.AOL, envop->entry(k + 1), D(k), d, D(k + 1), W(k + 1), D(k + 1)));
     }
-    MPSB_TRY(set_boundary(ctx, envop->entry(na), coef[np]));
-    // ---- right-to-left half sweep
+  } else {
+    for (int l = 0; l < np; ++l) {
+      MPSB_TRY(set_boundary(ctx, env[l]->entry(na), ONE));
+      MPSB_TRY(set_boundary(ctx, env[l]->entry(0), coef[l]));
+    }
+    MPSB_TRY(set_boundary(ctx, envop->entry(na), ONE));
+    MPSB_TRY(set_boundary(ctx, envop->entry(0), coef[np]));
+    for (int k = na - 1; k >= 1; --k) {
+      if (wait) MPSB_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, wait[k], 0));
+      for (int l = 0; l < np; ++l) {
+        MPSB_TRY(op_A3_R2(ctx, A[l]->site(k), env[l]->entry(k + 1), s.P[l], D(k) * d, D(k + 1), D(k + 1), ONE, ZERO));
+        MPSB_TRY(op_update_renv(ctx, Ain->site(k), s.P[l], env[l]->entry(k), D(k), D(k), d * D(k + 1)));
+      }
+      MPSB_TRY(op_prod_AOR(ctx, AH->site(k), H->site(k), envop->entry(k + 1), s.AOR, D(k), d, D(k + 1), W(k), W(k + 1), D(k + 1)));
+      MPSB_TRY(op_update_re(ctx, Ain->site(k), s.AOR, envop->entry(k), D(k), W(k), d, D(k + 1), D(k)));
+    }
+  }
+  return MPSB_OK;
+}
+
+// The half sweep of a sum stage (R->L when !right, L->R when right) writing A0 site by site;
+// `rec`, when given, gets one event per site recorded as soon as that site of A0 is final.
+static int sum_var_sweep(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* const* env, mpsb_env* envop, int numv,
+                         const mpsb_mps* const* A, const mpsb_mpo* H, const SweepScratch& s, const cudaEvent_t* rec) {
+  const int np = numv - 1, na = A0->na, d = A0->d;
+  const mpsb_mps* AH = A[np];
+  auto D = [&](int k) { return (int)A0->dims[k]; };
+  auto W = [&](int k) { return (int)H->w[k]; };
+  auto final_site = [&](int k) -> int {
+    if (rec) MPSB_CUDA_TRY(cudaEventRecord(rec[k], ctx->stream));
+    return MPSB_OK;
+  };
+  if (!right) {
     for (int k = na - 1; k >= 0; --k) {
       cd* out = A0->site(k);
       for (int l = 0; l < np; ++l) {
@@ -279,29 +313,17 @@ int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* 
       }
       MPSB_TRY(op_prod_AOR(ctx, AH->site(k), H->site(k), envop->entry(k + 1), s.AOR, D(k), d, D(k + 1), W(k), W(k + 1), D(k + 1)));
       MPSB_TRY(op_prod_LR_3_4(ctx, envop->entry(k), s.AOR, out, D(k), W(k), D(k), d, D(k + 1), ONE, np ? ONE : ZERO));
-      if (k == 0) break;
+      if (k == 0) {
+        MPSB_TRY(final_site(0));
+        break;
+      }
       MPSB_TRY(op_orth_right(ctx, out, D(k), d, D(k + 1)));
+      MPSB_TRY(final_site(k));
       for (int l = 0; l < np; ++l)
         MPSB_TRY(op_update_renv(ctx, out, s.P[l], env[l]->entry(k), D(k), D(k), d * D(k + 1)));
       MPSB_TRY(op_update_re(ctx, out, s.AOR, envop->entry(k), D(k), W(k), d, D(k + 1), D(k)));
     }
   } else {
-    // ---- right environments
-    for (int l = 0; l < np; ++l) {
-      MPSB_TRY(set_boundary(ctx, env[l]->entry(na), ONE));
-      for (int k = na - 1; k >= 1; --k) {
-        MPSB_TRY(op_A3_R2(ctx, A[l]->site(k), env[l]->entry(k + 1), s.P[l], D(k) * d, D(k + 1), D(k + 1), ONE, ZERO));
-        MPSB_TRY(op_update_renv(ctx, Ain->site(k), s.P[l], env[l]->entry(k), D(k), D(k), d * D(k + 1)));
-      }
-      MPSB_TRY(set_boundary(ctx, env[l]->entry(0), coef[l]));
-    }
-    MPSB_TRY(set_boundary(ctx, envop->entry(na), ONE));
-    for (int k = na - 1; k >= 1; --k) {
-      MPSB_TRY(op_prod_AOR(ctx, AH->site(k), H->site(k), envop->entry(k + 1), s.AOR, D(k), d, D(k + 1), W(k), W(k + 1), D(k + 1)));
-      MPSB_TRY(op_update_re(ctx, Ain->site(k), s.AOR, envop->entry(k), D(k), W(k), d, D(k + 1), D(k)));
-    }
-    MPSB_TRY(set_boundary(ctx, envop->entry(0), coef[np]));
-    // ---- left-to-right half sweep
     for (int k = 0; k < na; ++k) {
       cd* out = A0->site(k);
       for (int l = 0; l < np; ++l) {
@@ -310,14 +332,32 @@ int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* 
       }
       MPSB_TRY(op_prod_AOL(ctx, AH->site(k), H->site(k), envop->entry(k), s.AOL, D(k), d, D(k + 1), W(k), W(k + 1), D(k)));
       MPSB_TRY(op_prod_LR_4_3(ctx, s.AOL, envop->entry(k + 1), out, D(k), d, D(k + 1), W(k + 1), D(k + 1), ONE, np ? ONE : ZERO));
-      if (k == na - 1) break;
+      if (k == na - 1) {
+        MPSB_TRY(final_site(k));
+        break;
+      }
       MPSB_TRY(op_orth_left(ctx, out, D(k), d, D(k + 1), nullptr));
+      MPSB_TRY(final_site(k));
       for (int l = 0; l < np; ++l)
         MPSB_TRY(op_update_lenv(ctx, out, s.P[l], env[l]->entry(k + 1), D(k) * d, D(k + 1), D(k + 1), true));
       MPSB_TRY(op_update_le(ctx, out, s.AOL, envop->entry(k + 1), D(k), d, D(k + 1), W(k + 1), D(k + 1)));
     }
   }
   return MPSB_OK;
+}
+
+// compress_sum_var_apply_H_left! (src/compression.jl:889-944) when !right,
+// compress_sum_var_apply_H_right! (src/compression.jl:1007-1063) when right.
+// numv == 1 with coef {1} is compress_var_apply_H_left! (src/compression.jl:321-347).
+int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* const* env, mpsb_env* envop,
+                             const mpsb_mps* Ain, const cd* coef, int numv, const mpsb_mps* const* A,
+                             const mpsb_mpo* H) {
+  if (!ctx || !A0 || !envop || !Ain || !coef || !A || !H || numv < 1) return MPSB_ERR_INVALID_ARG;
+  MPSB_TRY(sum_var_check(A0, env, envop, Ain, numv, A, H));
+  SweepScratch s;
+  MPSB_TRY(sweep_scratch(ctx, A0, H, numv - 1, s));
+  MPSB_TRY(sum_var_init(ctx, right, env, envop, Ain, coef, numv, A, H, s, nullptr));
+  return sum_var_sweep(ctx, right, A0, env, envop, numv, A, H, s, nullptr);
 }
 
 int compress_var_apply_H_left(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain, const mpsb_mps* A,
@@ -467,10 +507,10 @@ int compress_sum_var_full(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const cd
   return site_lr(na - 1);
 }
 
-// RK4stp_apply_H_half! (src/timeevolution.jl:178-196)
-static int rk4_body(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
-                    mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3, mpsb_env* env1,
-                    mpsb_env* env2, mpsb_env* env3, mpsb_env* envop) {
+// RK4stp_apply_H_half! (src/timeevolution.jl:178-196), one stage after the other
+static int rk4_body_serial(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
+                           mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3,
+                           mpsb_env* env1, mpsb_env* env2, mpsb_env* env3, mpsb_env* envop) {
   MPSB_TRY(compress_var_apply_H_left(ctx, psi1, envop, psi, psi, H1));
   {
     mpsb_env* e[1] = {env1};
@@ -493,6 +533,118 @@ static int rk4_body(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo
   return MPSB_OK;
 }
 
+// Scratch for any of the four stages (three plain terms, the widest of the three operators);
+// slots only grow, so the pointers of the last call stay valid for all.
+static int sweep_scratch_all(mpsb_ctx* ctx, const mpsb_mps* A0, const mpsb_mpo* H1, const mpsb_mpo* H2,
+                             const mpsb_mpo* H3, SweepScratch& s) {
+  MPSB_TRY(sweep_scratch(ctx, A0, H1, 3, s));
+  MPSB_TRY(sweep_scratch(ctx, A0, H2, 3, s));
+  return sweep_scratch(ctx, A0, H3, 3, s);
+}
+
+// While alive, work is issued on the context's second lane (stream `side`, workspace ws_side).
+struct SideLane {
+  mpsb_ctx* c;
+  cudaStream_t saved;
+  explicit SideLane(mpsb_ctx* ctx) : c(ctx), saved(ctx->stream) {
+    c->stream = c->side;
+    std::swap(c->ws, c->ws_side);
+  }
+  ~SideLane() {
+    std::swap(c->ws, c->ws_side);
+    c->stream = saved;
+  }
+};
+
+static int ensure_events(mpsb_ctx* ctx, size_t n) {
+  while (ctx->events.size() < n) {
+    cudaEvent_t ev;
+    MPSB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    ctx->events.push_back(ev);
+  }
+  return MPSB_OK;
+}
+
+// An environment stack shaped like `like` whose storage is a context scratch slot.
+static int scratch_env(mpsb_ctx* ctx, Slot slot, const mpsb_env* like, mpsb_env& out) {
+  out = *like;
+  out.serial = 0;
+  return ensure_slot(ctx, slot, (size_t)like->total * sizeof(cd), &out.slab);
+}
+
+// The same four stages with each stage's environment initialisation (which reads the previous
+// stage's output site by site, in the order that stage finalises them) issued on the second
+// lane, waiting per site, so it runs beside the previous stage's sweep -- in particular beside
+// its QRs, which occupy one thread-block cluster.  Every computation is the one of the serial
+// body, so the results are identical.  Stages 2 and 4 use an internal envop, stage 3 env2 and
+// stage 4 an internal third plain-term environment, so that concurrent stages never share an
+// environment buffer.
+static int rk4_body_pipelined(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
+                              mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3,
+                              mpsb_env* env1, mpsb_env* env2, mpsb_env* env3, mpsb_env* envop) {
+  const int na = psi->na;
+  MPSB_TRY(ensure_events(ctx, (size_t)3 * na + 4));
+  cudaEvent_t* ev = ctx->events.data();
+  cudaEvent_t* site_ev[3] = {ev, ev + na, ev + 2 * na};
+  cudaEvent_t done[3] = {ev[3 * na], ev[3 * na + 1], ev[3 * na + 2]};
+  cudaEvent_t fork = ev[3 * na + 3];
+  mpsb_env envopB, envX;
+  MPSB_TRY(scratch_env(ctx, SLOT_PIPE_ENVOP, envop, envopB));
+  MPSB_TRY(scratch_env(ctx, SLOT_PIPE_ENV, env1, envX));
+
+  // stage descriptions: which half sweep, output, bra, terms, coefficients, operator, envs
+  const cd c1[1] = {ONE};
+  const cd c2[2] = {ONE, cmk(dt / 2, 0.0)};
+  const cd c3[2] = {ONE, cmk(dt, 0.0)};
+  const cd c4[4] = {cmk(-1.0 / 3, 0.0), cmk(1.0 / 3, 0.0), cmk(2.0 / 3, 0.0), cmk(1.0 / 3, 0.0)};
+  const mpsb_mps* t1[1] = {psi};
+  const mpsb_mps* t2[2] = {psi, psi1};
+  const mpsb_mps* t3[2] = {psi, psi2};
+  const mpsb_mps* t4[4] = {psi, psi1, psi2, psi3};
+  mpsb_env* e2[1] = {env1};
+  mpsb_env* e3[1] = {env2};
+  mpsb_env* e4[3] = {env1, env3, &envX};
+  struct Stage {
+    bool right; mpsb_mps* A0; const mpsb_mps* Ain; const cd* coef; int numv; const mpsb_mps* const* A;
+    const mpsb_mpo* H; mpsb_env* const* env; mpsb_env* envop;
+  };
+  const Stage st[4] = {{false, psi1, psi, c1, 1, t1, H1, nullptr, envop},
+                       {true, psi2, psi1, c2, 2, t2, H2, e2, &envopB},
+                       {false, psi3, psi2, c3, 2, t3, H2, e3, envop},
+                       {true, psi0, psi3, c4, 4, t4, H3, e4, &envopB}};
+  for (const Stage& g : st) MPSB_TRY(sum_var_check(g.A0, g.env, g.envop, g.Ain, g.numv, g.A, g.H));
+
+  SweepScratch sm;   // main lane scratch, sized for every stage
+  MPSB_TRY(sweep_scratch_all(ctx, psi, H1, H2, H3, sm));
+  MPSB_CUDA_TRY(cudaEventRecord(fork, ctx->stream));
+  MPSB_TRY(sum_var_init(ctx, st[0].right, st[0].env, st[0].envop, st[0].Ain, st[0].coef, st[0].numv, st[0].A, st[0].H, sm,
+                        nullptr));
+  for (int i = 0; i < 4; ++i) {
+    const Stage& g = st[i];
+    MPSB_TRY(sum_var_sweep(ctx, g.right, g.A0, g.env, g.envop, g.numv, g.A, g.H, sm, i < 3 ? site_ev[i] : nullptr));
+    if (i == 3) break;
+    const Stage& n = st[i + 1];
+    {
+      SideLane lane(ctx);
+      if (i == 0) MPSB_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, fork, 0));
+      SweepScratch ss;
+      MPSB_TRY(sweep_scratch_all(ctx, psi, H1, H2, H3, ss));
+      MPSB_TRY(sum_var_init(ctx, n.right, n.env, n.envop, n.Ain, n.coef, n.numv, n.A, n.H, ss, site_ev[i]));
+      MPSB_CUDA_TRY(cudaEventRecord(done[i], ctx->stream));
+    }
+    MPSB_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, done[i], 0));
+  }
+  return MPSB_OK;
+}
+
+static int rk4_body(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
+                    mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3, mpsb_env* env1,
+                    mpsb_env* env2, mpsb_env* env3, mpsb_env* envop) {
+  if (ctx->pipeline && ctx->side)
+    return rk4_body_pipelined(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
+  return rk4_body_serial(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
+}
+
 int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3, mpsb_mps* psi0,
              mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3, mpsb_env* env1, mpsb_env* env2,
              mpsb_env* env3, mpsb_env* envop) {
@@ -502,7 +654,7 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
     return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
   int64_t dtbits;
   std::memcpy(&dtbits, &dt, sizeof(dt));
-  std::vector<int64_t> key = {1, dtbits, H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial,
+  std::vector<int64_t> key = {ctx->pipeline ? 2 : 1, dtbits, H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial,
                               psi1->serial, psi2->serial, psi3->serial, env1->serial, env2->serial,
                               env3->serial, envop->serial};
   auto& ent = ctx->graphs_cache[key];
@@ -521,13 +673,13 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
     return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
   }
   const int64_t gen0 = ctx->ws_generation;
-  const int64_t l0 = ctx->ws.launches;
-  ctx->ws.capturing = true;
+  const int64_t l0 = ctx->ws.launches + ctx->ws_side.launches;
+  ctx->ws.capturing = ctx->ws_side.capturing = true;
   MPSB_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   int st = rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
   cudaGraph_t g = nullptr;
   cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
-  ctx->ws.capturing = false;
+  ctx->ws.capturing = ctx->ws_side.capturing = false;
   if (st != MPSB_OK) {
     if (g) cudaGraphDestroy(g);
     return st;
@@ -545,7 +697,7 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
   }
   ent.exec = exec;
   ent.generation = gen0;
-  ent.launches = ctx->ws.launches - l0;
+  ent.launches = ctx->ws.launches + ctx->ws_side.launches - l0;
   MPSB_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
   return MPSB_OK;
 }

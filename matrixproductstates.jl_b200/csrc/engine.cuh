@@ -14,6 +14,12 @@ struct mpsb_ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   mpsb::Workspace ws;
+  // second lane of the RK4 step: the next stage's environment initialisation runs on `side`
+  // with its own scratch and split-K workspace (swapped into `ws`/`stream` while it issues)
+  cudaStream_t side = nullptr;
+  mpsb::Workspace ws_side;
+  std::vector<cudaEvent_t> events;   // per-site / fork / join events, created on first use
+  bool pipeline = true;
   bool graphs = true;
   int64_t ws_generation = 0;   // bumped whenever a scratch buffer is reallocated
   double* d_scalars = nullptr; // small device scratch for norms (64 doubles)
@@ -71,7 +77,7 @@ namespace mpsb {
 // named scratch slots in Workspace::named
 enum Slot {
   SLOT_T = 0, SLOT_AOR, SLOT_G1, SLOT_AOL, SLOT_P0, SLOT_P1, SLOT_P2, SLOT_ENV0, SLOT_ENV1,
-  SLOT_MISC, SLOT_SUMENV, SLOT_GSENV, SLOT_GSVEC, SLOT_COUNT
+  SLOT_MISC, SLOT_SUMENV, SLOT_GSENV, SLOT_GSVEC, SLOT_PIPE_ENVOP, SLOT_PIPE_ENV, SLOT_COUNT
 };
 
 int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out);

@@ -35,6 +35,7 @@ SIGNATURES = {
     "mpsb_sync": ([_vp], _i),
     "mpsb_ctx_set_stream": ([_vp, _vp], _i),
     "mpsb_ctx_set_graphs": ([_vp, _i], _i),
+    "mpsb_ctx_set_pipeline": ([_vp, _i], _i),
     "mpsb_ctx_launch_count": ([_vp, _pi64], _i),
     "mpsb_mps_create": ([_vp, _i, _i, _pi64, _pvp], _i),
     "mpsb_mps_destroy": ([_vp], _i),

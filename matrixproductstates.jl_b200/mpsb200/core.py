@@ -45,6 +45,11 @@ class Context:
     def set_graphs(self, enable):
         _lib.call("mpsb_ctx_set_graphs", self.h, 1 if enable else 0)
 
+    def set_pipeline(self, enable):
+        """Overlap each RK4 stage's environment initialisation with the previous stage's sweep
+        on a second stream (default on; identical results)."""
+        _lib.call("mpsb_ctx_set_pipeline", self.h, 1 if enable else 0)
+
     def set_stream(self, stream_ptr):
         _lib.call("mpsb_ctx_set_stream", self.h, C.c_void_p(stream_ptr or 0))
 

@@ -216,6 +216,25 @@ def test_graph_replay_is_bitwise_eager(gpu_ctx):
     assert np.array_equal(outs[0], outs[1])
 
 
+@pytest.mark.parametrize("graphs", [False, True])
+def test_pipelined_rk4_is_bitwise_serial(gpu_ctx, graphs):
+    """The two-stream RK4 step (each stage's environment initialisation beside the previous
+    stage's sweep) computes exactly what the serial step computes, eagerly and replayed."""
+    from mpsb200 import drivers as GDR, models as GM
+    p = GM.WaveguideChain(10, gam_eg=0.1, omega=0.5, gam_phi=0.1)
+    outs = []
+    gpu_ctx.set_graphs(graphs)
+    for pipe in (False, True):
+        gpu_ctx.set_pipeline(pipe)
+        b = GDR.DensityBuffers(p, 32, 0.005, 8, gpu_ctx)
+        for _ in range(6):
+            b.step()
+        outs.append(np.concatenate([s.ravel() for s in b.rho.sites()]))
+    gpu_ctx.set_pipeline(True)
+    gpu_ctx.set_graphs(True)
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_rk4_rho_chi512_blocked_qr(gpu_ctx):
     """The chi <= 512 configuration at reduced length (N=10, d=4, w=8): a random chi=64 state
     (mpsrandom semantics, normalised) expanded to chi=512; its 1024 x 512 and 2048 x 256 QRs
