@@ -291,6 +291,21 @@ def time_qr(ctx, torch, stream):
     return 16.0 * (m * n * n - n ** 3 / 3.0), e0.elapsed_time(e1) / 1e3 / reps, m, n
 
 
+def run_serving():
+    """p50/p99 job latency of a bounded sample of the mixed serving stream: 24 seeded Poisson
+    arrivals at 200 jobs/s, 70% trajectories (N 20..40, chi 16/32/64, d=2, w=4) and 30%
+    density matrices (N 8..16, chi 16/32, d=4, w=8), 10..30 RK4 steps each, up to 8 jobs on the
+    device at once (the configuration's full sizes and 100-500 steps would run for minutes)."""
+    from mpsb200 import serve as S
+    jobs = S.poisson_jobs(24, 200.0, 11)
+    done, st = S.Server(max_jobs=8).run(jobs)
+    return {"jobs": st["jobs"], "arrival_rate_per_s": 200.0, "slots": 8,
+            "latency_p50_ms": 1e3 * st["latency_p50_s"], "latency_p99_ms": 1e3 * st["latency_p99_s"],
+            "queue_p50_ms": 1e3 * st["queue_p50_s"], "site_updates_per_s": st["site_updates_per_s"],
+            "wall_s": st["wall_s"],
+            "sample": "24 jobs: 70% trajectories N 20..40 chi<=64, 30% rho N 8..16 chi<=32, 10..30 steps"}
+
+
 def run_ours(args, rank, world, local_rank, dist):
     import numpy as np
     import torch
@@ -394,6 +409,9 @@ def run_ours(args, rank, world, local_rank, dist):
                      "per_launch": "flop-weighted mean over the %d GEMM shapes of an interior site "
                                    "(chi=128, d=4, w=8): %.3e flops in %.1f us; traffic = the prod_LR launch "
                                    "(M=128, N=512, K=1024) dram read+write (ncu)" % (ncalls, gflops, gsecs * 1e6)}
+    serving = None
+    if world == 1 and not args.no_serve:
+        serving = run_serving()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
@@ -409,6 +427,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16,
                 "steps": ke},
         "check": {"trace_rho": tr.real, "max_see": float(np.max(see.real))},
+        "serving": serving,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         model, cores = cpu_info()
@@ -427,6 +446,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream sample")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

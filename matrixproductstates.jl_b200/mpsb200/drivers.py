@@ -42,41 +42,48 @@ class TrajectoryBuffers:
         return K.normalize_lo_(self.A_coh)
 
 
+def trajectory_decision(b, i, p_coh, r1, r2, rec):
+    """The jump branch of step i (examples/spin_model_quantum_trajectory_rk4.jl:105-190): keep
+    the coherent state when r1[i] < p_coh, else pick a local decay or a waveguide jump from the
+    accumulated probabilities with r2[i] and apply it; jumps are appended to rec["jumps"]."""
+    p, dt, na = b.p, b.dt, b.p.na
+    if r1[i] < p_coh:
+        b.A.copy_from(b.A_coh)
+        return
+    K.compress_var_apply_H_(b.A_r, b.envop_jump, b.A, b.A, b.jumpright, 1)
+    p_r = K.normalize_lo_(b.A_r)
+    K.compress_var_apply_H_(b.A_l, b.envop_jump, b.A, b.A, b.jumpleft, 1)
+    p_l = K.normalize_lo_(b.A_l)
+    epop = K.measure_local(b.A, Mo.E_E)
+    p_acc = np.zeros(na + 3)
+    for j in range(na):
+        p_acc[j + 1] = p_acc[j] + dt * p.gam_eg * epop[j]
+    p_acc[na + 1] = p_acc[na] + dt * p_r
+    p_acc[na + 2] = p_acc[na + 1] + dt * p_l
+    p_sum = p_acc[-1]
+    p_acc = p_acc / p_acc[-1]
+    if r2[i] < p_acc[na]:
+        for j in range(na):
+            if r2[i] < p_acc[j + 1]:
+                K.apply_site_operator_(b.A, j + 1, Mo.SM)
+                K.leftorthonormalizationQR_(b.A)
+                rec["jumps"].append((i, "local", j + 1, p_coh, p_sum))
+                break
+    elif r2[i] < p_acc[na + 1]:
+        b.A.copy_from(b.A_r)
+        rec["jumps"].append((i, "right", 0, p_coh, p_sum))
+    else:
+        b.A.copy_from(b.A_l)
+        rec["jumps"].append((i, "left", 0, p_coh, p_sum))
+
+
 def run_trajectory(p, dmax, dt, nsteps, r1, r2, measure_int=10, ctx=None):
     b = TrajectoryBuffers(p, dmax, dt, ctx)
-    na = p.na
     rec = {"p_coh": np.zeros(nsteps), "jumps": [], "e_pop": [K.measure_local(b.A, Mo.E_E)]}
     for i in range(nsteps):
         p_coh = b.coherent_step()
         rec["p_coh"][i] = p_coh
-        if r1[i] < p_coh:
-            b.A.copy_from(b.A_coh)
-        else:
-            K.compress_var_apply_H_(b.A_r, b.envop_jump, b.A, b.A, b.jumpright, 1)
-            p_r = K.normalize_lo_(b.A_r)
-            K.compress_var_apply_H_(b.A_l, b.envop_jump, b.A, b.A, b.jumpleft, 1)
-            p_l = K.normalize_lo_(b.A_l)
-            epop = K.measure_local(b.A, Mo.E_E)
-            p_acc = np.zeros(na + 3)
-            for j in range(na):
-                p_acc[j + 1] = p_acc[j] + dt * p.gam_eg * epop[j]
-            p_acc[na + 1] = p_acc[na] + dt * p_r
-            p_acc[na + 2] = p_acc[na + 1] + dt * p_l
-            p_sum = p_acc[-1]
-            p_acc = p_acc / p_acc[-1]
-            if r2[i] < p_acc[na]:
-                for j in range(na):
-                    if r2[i] < p_acc[j + 1]:
-                        K.apply_site_operator_(b.A, j + 1, Mo.SM)
-                        K.leftorthonormalizationQR_(b.A)
-                        rec["jumps"].append((i, "local", j + 1, p_coh, p_sum))
-                        break
-            elif r2[i] < p_acc[na + 1]:
-                b.A.copy_from(b.A_r)
-                rec["jumps"].append((i, "right", 0, p_coh, p_sum))
-            else:
-                b.A.copy_from(b.A_l)
-                rec["jumps"].append((i, "left", 0, p_coh, p_sum))
+        trajectory_decision(b, i, p_coh, r1, r2, rec)
         if (i + 1) % measure_int == 0:
             rec["e_pop"].append(K.measure_local(b.A, Mo.E_E))
     rec["e_pop"] = np.array(rec["e_pop"])
