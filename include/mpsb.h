@@ -225,6 +225,17 @@ int mpsb_op_prod_AOR_noalloc(void* stream, const void* A, const void* O, const v
 int mpsb_compression_svd(mpsb_ctx* ctx, const mpsb_mps* in, int dmax, double tol, mpsb_mps** out,
                          double* err_glob, double* err_trim, double* ent_ent);
 
+/* compress_var_apply_H_two_site(Ain, A, H, maxsweeps, svd_tol, dims, dlim)  src/compression.jl:355-411
+ * Two-site variational compression of H*A (guess Ain, left canonical) with a thin SVD of each
+ * pair tensor truncated by the compressionSVD! rule; the bond dims adapt (<= dlim), so the
+ * result is a new handle *out (its dims are the reference's updated `dims`).  The reference's
+ * version calls the undefined `svdecon` and contracts its stored-conjugated left environment
+ * unconjugated; this one uses the thin SVD and the single-site path's conjugation.
+ * compress_var_two_site (src/compression.jl:110-165) is this call with an identity MPO. */
+int mpsb_compress_var_apply_H_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A,
+                                       const mpsb_mpo* H, int maxsweeps, double svd_tol, int dlim,
+                                       mpsb_mps** out);
+
 /* svd(M) as compressionSVD! calls it (src/compression.jl:1296): thin SVD X = U diag(S) V^H of a
  * device m x n column-major matrix, k = min(m, n); U (m x k) and V (n x k) device, S (k) host,
  * singular values descending.  One-sided Jacobi (relative accuracy); phases of the singular

@@ -676,6 +676,22 @@ int mpsb_compression_svd(mpsb_ctx* ctx, const mpsb_mps* in, int dmax, double tol
   return sync(ctx);
 }
 
+int mpsb_compress_var_apply_H_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, const mpsb_mpo* H,
+                                       int maxsweeps, double svd_tol, int dlim, mpsb_mps** out) {
+  MPSB_TRY(bind(ctx));
+  if (!out) return MPSB_ERR_INVALID_ARG;
+  std::vector<int64_t> dims, offs;
+  cd* sites = nullptr;
+  MPSB_TRY(compress_two_site(ctx, Ain, A, H, maxsweeps, svd_tol, dlim, dims, offs, &sites));
+  mpsb_mps* R = nullptr;
+  MPSB_TRY(mpsb_mps_create(ctx, A->na, A->d, dims.data(), &R));
+  for (int k = 0; k < A->na; ++k)
+    MPSB_CUDA_TRY(cudaMemcpyAsync(R->site(k), sites + offs[k], R->site_elems(k) * sizeof(cd), cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+  *out = R;
+  return sync(ctx);
+}
+
 int mpsb_op_svd(mpsb_ctx* ctx, const void* X, void* U, double* S, void* V, int m, int n) {
   MPSB_TRY(bind(ctx));
   if (!X || !U || !S || !V || m < 1 || n < 1) return MPSB_ERR_DIMENSION;

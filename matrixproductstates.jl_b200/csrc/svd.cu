@@ -318,3 +318,164 @@ int compression_svd(mpsb_ctx* ctx, const mpsb_mps* in, int dmax, double tol, std
 }
 
 }  // namespace mpsb
+
+// ---- two-site variational compression with SVD truncation -------------------------------
+namespace mpsb {
+namespace {
+
+// D[:, j] = s[j] * ... : out (k x n) = diag(s) V^H for the first k columns of V (n x kv)
+__global__ void sv_adjoint_kernel(int k, int n, const cd* V, int64_t ldv, const double* s, cd* out) {
+  const int64_t total = (int64_t)k * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e % k), c = (int)(e / k);
+    const cd v = cconj(V[(int64_t)r * ldv + c]);
+    out[e] = s ? cmk(v.x * s[r], v.y * s[r]) : v;
+  }
+}
+
+int truncation_rule(const std::vector<double>& S, int k, double tol, int dlim) {
+  int kp = 0;
+  double stot = 0.0;
+  while (kp < k && S[kp] > 0) {
+    stot += S[kp] * S[kp];
+    ++kp;
+  }
+  if (kp == 0) return 0;
+  int below = 0;
+  double cum = 0.0;
+  for (int j = 0; j < kp; ++j) {
+    cum += S[j] * S[j] / stot;
+    if (cum < 1.0 - tol) ++below;
+  }
+  return std::min(std::min(below + 1, dlim), kp);
+}
+
+}  // namespace
+
+// compress_var_apply_H_two_site (src/compression.jl:355-411): maxsweeps sweep pairs of the
+// two-site variational compression of H A with guess Ain; each pair's effective tensor
+// av[a0,s1,s2,b0] = sum L[a,w,a0]* A1[a,t1,c] O1[w,s1,v,t1] A2[c,t2,b] O2[v,s2,u,t2] R[b,u,b0]
+// (the left environment conjugated as every single-site contraction uses it) is split by a
+// thin SVD, truncated by the compressionSVD! rule (svd_tol, dlim), the bond updated.  Bond
+// dims change; the result lands in context scratch (site k at offs[k]) with dims_out.
+int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, const mpsb_mpo* H, int maxsweeps,
+                      double svd_tol, int dlim, std::vector<int64_t>& dims_out, std::vector<int64_t>& offs,
+                      cd** sites) {
+  if (!ctx || !Ain || !A || !H || maxsweeps < 1 || dlim < 1 || !(svd_tol >= 0)) return MPSB_ERR_INVALID_ARG;
+  const int na = A->na, d = A->d;
+  if (Ain->na != na || Ain->d != d || H->na != na || H->d != d || na < 2) return MPSB_ERR_DIMENSION;
+  cudaStream_t st = ctx->stream;
+  std::vector<int64_t> dims = Ain->dims, cap(na + 1);
+  for (int k = 0; k <= na; ++k) {   // capacity of bond k: the dims rule bound with dlim
+    int64_t c = dlim, pl = 1, pr = 1;
+    for (int i = 0; i < k && pl < c; ++i) pl *= d;
+    for (int i = k; i < na && pr < c; ++i) pr *= d;
+    cap[k] = std::max<int64_t>(dims[k], std::min(c, std::min(pl, pr)));
+  }
+  auto DA = [&](int k) { return (int)A->dims[k]; };
+  auto W = [&](int k) { return (int)H->w[k]; };
+  // scratch: A0 sites at capacity, FL and FR stacks, the pair tensors and the SVD factors
+  offs.assign(na, 0);
+  int64_t tot = 0, envtot = 0, pairmax = 1, aor = 1;
+  std::vector<int64_t> eoff(na + 1);
+  for (int k = 0; k < na; ++k) {
+    offs[k] = tot;
+    tot += cap[k] * d * cap[k + 1];
+  }
+  for (int k = 0; k <= na; ++k) {
+    eoff[k] = envtot;
+    envtot += (int64_t)DA(k) * W(k) * cap[k];
+  }
+  for (int k = 0; k + 1 < na; ++k) {
+    pairmax = std::max<int64_t>(pairmax, cap[k] * d * d * cap[k + 2]);
+    aor = std::max<int64_t>(aor, (int64_t)DA(k) * W(k) * d * d * cap[k + 2]);
+    aor = std::max<int64_t>(aor, (int64_t)DA(k + 1) * W(k + 1) * d * cap[k + 2]);
+  }
+  for (int k = 0; k < na; ++k) {
+    aor = std::max<int64_t>(aor, (int64_t)DA(k) * W(k) * d * cap[k + 1]);
+    aor = std::max<int64_t>(aor, (int64_t)cap[k] * d * DA(k + 1) * W(k + 1));
+  }
+  const size_t need = (size_t)tot + 2 * envtot + 2 * aor + 3 * pairmax + pairmax / 2 + 64;
+  cd* base = nullptr;
+  MPSB_TRY(ensure_slot(ctx, SLOT_MISC, need * sizeof(cd), &base));
+  cd* A0 = base;
+  cd* FLb = A0 + tot;
+  cd* FRb = FLb + envtot;
+  cd* X = FRb + envtot;
+  cd* Y = X + aor;
+  cd* av = Y + aor;
+  cd* U = av + pairmax;
+  cd* V = U + pairmax;
+  double* dS = reinterpret_cast<double*>(V + pairmax);
+  auto FL = [&](int k) { return FLb + eoff[k]; };
+  auto FR = [&](int k) { return FRb + eoff[k]; };
+  auto site0 = [&](int k) { return A0 + offs[k]; };
+  // A0 starts as the guess (dims of Ain)
+  for (int k = 0; k < na; ++k)
+    MPSB_CUDA_TRY(cudaMemcpyAsync(site0(k), Ain->site(k), Ain->site_elems(k) * sizeof(cd), cudaMemcpyDeviceToDevice, st));
+  const cd ONE_ = cmk(1.0, 0.0);
+  MPSB_TRY(set_boundary(ctx, FL(0), ONE_));
+  for (int k = 0; k < na - 2; ++k) {   // FL[k+1] = update_le(Ain[k], H[k], A[k], FL[k])
+    MPSB_TRY(op_prod_AOL(ctx, A->site(k), H->site(k), FL(k), Y, DA(k), d, DA(k + 1), W(k), W(k + 1), (int)dims[k]));
+    MPSB_TRY(op_update_le(ctx, site0(k), Y, FL(k + 1), (int)dims[k], d, DA(k + 1), W(k + 1), (int)dims[k + 1]));
+  }
+  MPSB_TRY(set_boundary(ctx, FR(na), ONE_));
+  std::vector<double> S;
+  // the pair tensor of sites (j, j+1) into av: (dims[j] d) x (d dims[j+2])
+  auto pair = [&](int j) -> int {
+    const int b0 = (int)dims[j + 2], a0 = (int)dims[j];
+    // X[c, v, s2, b0] = prod_AOR(A[j+1], H[j+1], FR[j+2])
+    MPSB_TRY(op_prod_AOR(ctx, A->site(j + 1), H->site(j + 1), FR(j + 2), X, DA(j + 1), d, DA(j + 2), W(j + 1), W(j + 2), b0));
+    // Y[a, w, s1, (s2 b0)] = prod_AOR(A[j], H[j], X as R[c, v, (s2 b0)])
+    MPSB_TRY(op_prod_AOR(ctx, A->site(j), H->site(j), X, Y, DA(j), d, DA(j + 1), W(j), W(j + 1), d * b0));
+    // av[a0, s1, (s2 b0)] = sum_{a, w} conj(L[a, w, a0]) Y[a, w, s1, (s2 b0)]
+    return op_prod_LR_3_4(ctx, FL(j), Y, av, DA(j), W(j), a0, d, d * b0, ONE_, cmk(0.0, 0.0));
+  };
+  auto svd_pair = [&](int j, int& k) -> int {
+    const int m = (int)dims[j] * d, n = d * (int)dims[j + 2];
+    k = std::min(m, n);
+    S.assign(k, 0.0);
+    return svd_launch(m, n, av, 1, m, U, 1, m, S.data(), V, 1, n, &ctx->ws, st);
+  };
+  int k = 0, dnew = 1;
+  for (int sweep = 0; sweep < maxsweeps; ++sweep) {
+    for (int j = na - 2; j >= 0; --j) {   // sweep left: pairs (j, j+1), site j+1 becomes V'
+      MPSB_TRY(pair(j));
+      MPSB_TRY(svd_pair(j, k));
+      dnew = truncation_rule(S, k, svd_tol, dlim);
+      if (dnew == 0) { set_last_message("two-site compression: zero pair tensor"); return MPSB_ERR_NONFINITE; }
+      dims[j + 1] = dnew;
+      const int n = d * (int)dims[j + 2];
+      count_launch(&ctx->ws);
+      sv_adjoint_kernel<<<148 * 2, 256, 0, st>>>(dnew, n, V, n, nullptr, site0(j + 1));
+      MPSB_CUDA_TRY(cudaGetLastError());
+      // FR[j+1] = update_re(A0[j+1], H[j+1], A[j+1], FR[j+2])
+      MPSB_TRY(op_prod_AOR(ctx, A->site(j + 1), H->site(j + 1), FR(j + 2), X, DA(j + 1), d, DA(j + 2), W(j + 1),
+                           W(j + 2), (int)dims[j + 2]));
+      MPSB_TRY(op_update_re(ctx, site0(j + 1), X, FR(j + 1), DA(j + 1), W(j + 1), d, (int)dims[j + 2], dnew));
+    }
+    for (int j = 0; j <= na - 2; ++j) {   // sweep right: site j becomes U
+      MPSB_TRY(pair(j));
+      MPSB_TRY(svd_pair(j, k));
+      dnew = truncation_rule(S, k, svd_tol, dlim);
+      if (dnew == 0) { set_last_message("two-site compression: zero pair tensor"); return MPSB_ERR_NONFINITE; }
+      dims[j + 1] = dnew;
+      const int m = (int)dims[j] * d;
+      MPSB_CUDA_TRY(cudaMemcpyAsync(site0(j), U, (size_t)m * dnew * sizeof(cd), cudaMemcpyDeviceToDevice, st));
+      // FL[j+1] = update_le(A0[j], H[j], A[j], FL[j])
+      MPSB_TRY(op_prod_AOL(ctx, A->site(j), H->site(j), FL(j), Y, DA(j), d, DA(j + 1), W(j), W(j + 1), (int)dims[j]));
+      MPSB_TRY(op_update_le(ctx, site0(j), Y, FL(j + 1), (int)dims[j], d, DA(j + 1), W(j + 1), dnew));
+    }
+    // last site: diag(S) V' of the last pair
+    const int n = d * (int)dims[na];
+    MPSB_CUDA_TRY(cudaMemcpyAsync(dS, S.data(), dnew * sizeof(double), cudaMemcpyHostToDevice, st));
+    count_launch(&ctx->ws);
+    sv_adjoint_kernel<<<148 * 2, 256, 0, st>>>(dnew, n, V, n, dS, site0(na - 1));
+    MPSB_CUDA_TRY(cudaGetLastError());
+  }
+  dims_out = dims;
+  *sites = A0;
+  return MPSB_OK;
+}
+
+}  // namespace mpsb

@@ -479,12 +479,35 @@ def compressionSVD_(mps, dmax, tol=1e-15):
     ee = np.zeros(mps.na)
     _lib.call("mpsb_compression_svd", mps.ctx.h, mps.h, int(dmax), float(tol), C.byref(out), C.byref(eg),
               _dptr(et), _dptr(ee))
+    return _wrap_new_mps(out, mps.ctx, mps.na, mps.d), eg.value, et, ee
+
+
+def _wrap_new_mps(h, ctx, na, d):
     new = MPS.__new__(MPS)
-    new.ctx, new.na, new.d, new.h = mps.ctx, mps.na, mps.d, out
-    info = np.zeros(mps.na + 1, dtype=np.int64)
-    _lib.call("mpsb_mps_info", out, None, None, info.ctypes.data_as(C.POINTER(C.c_int64)))
+    new.ctx, new.na, new.d, new.h = ctx, na, d, h
+    info = np.zeros(na + 1, dtype=np.int64)
+    _lib.call("mpsb_mps_info", h, None, None, info.ctypes.data_as(C.POINTER(C.c_int64)))
     new.dims = [int(x) for x in info]
-    return new, eg.value, et, ee
+    return new
+
+
+def compress_var_apply_H_two_site(Ain, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:355-411: two-site variational compression of H*A with SVD truncation
+    (bonds adapt up to dlim).  Returns the new MPS; `dims` (a list) is updated in place like
+    the reference's."""
+    out = C.c_void_p()
+    _lib.call("mpsb_compress_var_apply_H_two_site", Ain.ctx.h, Ain.h, A.h, H.h, int(maxsweeps), float(svd_tol),
+              int(dlim), C.byref(out))
+    new = _wrap_new_mps(out, Ain.ctx, Ain.na, Ain.d)
+    dims[:] = new.dims
+    return new
+
+
+def compress_var_two_site(Ain, A, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:110-165: the same compression of A itself (an identity operator)."""
+    ident = np.eye(A.d, dtype=CT).reshape(1, A.d, 1, A.d)
+    Id = MPO.from_sites([ident] * A.na, A.ctx)
+    return compress_var_apply_H_two_site(Ain, A, Id, maxsweeps, svd_tol, dims, dlim)
 
 
 # ------------------------------------------------------------------ norms, gauge, observables

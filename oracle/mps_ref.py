@@ -756,5 +756,48 @@ def compressionSVD_(mps, dmax, tol=1e-15):
     return err_glob, err_trim, ent_ent
 
 
+def _trunc_rule(s, tol, dlim):
+    s = s[s > 0]
+    stot = np.sum(s ** 2)
+    return min(int(np.sum(np.cumsum(s ** 2 / stot) < 1 - tol)) + 1, dlim, len(s))
+
+
+def compress_var_apply_H_two_site(Ain, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:355-411 with its `svdecon` (undefined in the reference) as the thin
+    SVD, and the pair tensor contracted with the conjugated left environment like every
+    single-site contraction: av = sum conj(L) A1 O1 A2 O2 R.  dims is updated in place."""
+    na = len(Ain)
+    FL, FR = [None] * na, [None] * na
+    FL[0] = np.ones((1, 1, 1), dtype=CT)
+    for jj in range(na - 2):
+        FL[jj + 1] = update_le_full(Ain[jj], H[jj], A[jj], FL[jj])
+    FR[na - 1] = np.ones((1, 1, 1), dtype=CT)
+    A0 = [None] * na
+    d = A[0].shape[1]
+
+    def pair(j):
+        X = prod_AOR(A[j + 1], H[j + 1], FR[j + 1])                       # [c, v, s2, b0]
+        R2 = X.reshape(X.shape[0], X.shape[1], -1, order="F")              # [c, v, (s2 b0)]
+        Y = prod_AOR(A[j], H[j], R2)                                       # [a, w, s1, (s2 b0)]
+        av = np.einsum("awx,awsy->xsy", FL[j].conj(), Y)
+        return av.reshape(av.shape[0] * d, -1, order="F")
+
+    for _ in range(maxsweeps):
+        for j in range(na - 2, -1, -1):
+            u, s, vh = np.linalg.svd(pair(j), full_matrices=False)
+            dn = _trunc_rule(s, svd_tol, dlim)
+            dims[j + 1] = dn
+            A0[j + 1] = jr(vh[:dn, :], dn, d, dims[j + 2])
+            FR[j] = update_re_full(A0[j + 1], H[j + 1], A[j + 1], FR[j + 1])
+        for j in range(na - 1):
+            u, s, vh = np.linalg.svd(pair(j), full_matrices=False)
+            dn = _trunc_rule(s, svd_tol, dlim)
+            dims[j + 1] = dn
+            A0[j] = jr(u[:, :dn], dims[j], d, dn)
+            FL[j + 1] = update_le_full(A0[j], H[j], A[j], FL[j])
+        A0[na - 1] = jr(np.diag(s[:dn]) @ vh[:dn, :], dn, d, dims[na])
+    return A0
+
+
 def copy_mps(mps):
     return [np.array(a, dtype=CT, copy=True) for a in mps]

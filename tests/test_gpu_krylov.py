@@ -160,3 +160,29 @@ def test_compression_svd_matches_oracle(gpu_ctx, dmax, tol):
     assert np.abs(get - et).max() < 1e-12
     assert np.abs(gee - ee).max() < 1e-10
     assert 1 - fidelity(gnew.sites(), B) < 1e-12
+
+
+@pytest.mark.parametrize("dlim,tol,sweeps", [(16, 1e-14, 2), (6, 1e-10, 2), (12, 1e-3, 1)])
+def test_two_site_compression_matches_oracle(gpu_ctx, dlim, tol, sweeps):
+    """compress_var_apply_H_two_site / compress_var_two_site (the two-site SVD sweeps): adapted
+    bond dims and the compressed state (singular vectors are unique only up to phases)."""
+    import mpsb200 as K
+    na = 9
+    rng = np.random.default_rng(50)
+    A, dims = R.mpsrandom(na, 8, 2, rng)
+    H = OM.sm_hamiltonian(OM.SpinChain(na, omega=0.5), 1.0, 0.05, 0.0)
+    dd = list(dims)
+    ref = R.compress_var_apply_H_two_site(R.copy_mps(A), A, H, sweeps, tol, dd, dlim)
+    gA = K.MPS.from_sites(A, gpu_ctx)
+    gd = list(dims)
+    got = K.compress_var_apply_H_two_site(gA, gA, K.MPO.from_sites(H, gpu_ctx), sweeps, tol, gd, dlim)
+    assert gd == dd and got.dims == dd
+    assert 1 - fidelity(got.sites(), ref) < 1e-10
+    assert abs(R.scal_prod(got.sites(), got.sites()) / R.scal_prod(ref, ref) - 1) < 1e-10
+    # the plain (operator-free) form
+    ident = [np.eye(2, dtype=np.complex128).reshape(1, 2, 1, 2)] * na
+    dd2 = list(dims)
+    ref2 = R.compress_var_apply_H_two_site(R.copy_mps(A), A, ident, 1, 1e-14, dd2, dlim)
+    gd2 = list(dims)
+    got2 = K.compress_var_two_site(gA, gA, 1, 1e-14, gd2, dlim)
+    assert gd2 == dd2 and 1 - fidelity(got2.sites(), ref2) < 1e-10

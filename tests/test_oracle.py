@@ -354,3 +354,18 @@ def test_compression_svd_rule_and_exactness():
     assert max(c.shape[2] for c in C) <= 5
     assert np.all(et2 >= 0) and et2.max() > 0
     assert abs(ee2[-1] - ee[-1]) < 1e-12   # the first site processed sees the untruncated spectrum
+
+
+def test_two_site_compression_exact_at_full_bond_dimension():
+    """compress_var_apply_H_two_site (src/compression.jl:355-411, with a thin SVD for its
+    undefined svdecon): with dlim at the full bond dimension it reproduces H*A, and the bonds
+    grow from the guess's dims to what H*A needs."""
+    na = 8
+    rng = np.random.default_rng(3)
+    A, dims = R.mpsrandom(na, 8, 2, rng)
+    H = M.sm_hamiltonian(M.SpinChain(na, omega=0.5), 1.0, 0.05, 0.0)
+    dd = list(dims)
+    out = R.compress_var_apply_H_two_site(R.copy_mps(A), A, H, 2, 1e-14, dd, 16)
+    want = D.mpo_to_dense(H) @ D.mps_to_dense(A)
+    assert np.linalg.norm(D.mps_to_dense(out) - want) < 1e-12 * np.linalg.norm(want)
+    assert dd == [1, 2, 4, 8, 16, 8, 4, 2, 1]
