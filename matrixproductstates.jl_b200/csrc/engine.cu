@@ -160,12 +160,14 @@ int op_update_lenv(mpsb_ctx* ctx, const cd* A0, const cd* AL, cd* env, int lead,
   return run_gemm(ctx, g);
 }
 
-// QR through the context's workspace; a reallocated QR scratch invalidates captured graphs
+// QR through the context's workspace; a reallocated QR or split-K scratch (the blocked QR's
+// trailing GEMMs may split K) invalidates captured graphs
 int run_qr(mpsb_ctx* ctx, const QrProblem& p) {
   void* before = ctx->ws.qr.p;
+  void* before_sk = ctx->ws.splitk.p;
   count_launch(&ctx->ws);
   int st = qr_launch(p, &ctx->ws, ctx->stream);
-  if (ctx->ws.qr.p != before) ctx->ws_generation++;
+  if (ctx->ws.qr.p != before || ctx->ws.splitk.p != before_sk) ctx->ws_generation++;
   return st;
 }
 

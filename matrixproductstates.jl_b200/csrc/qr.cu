@@ -10,6 +10,18 @@
 // sign / phase rule above is what must match LAPACK, and it also fixes the "junk" columns of
 // zero-padded (rank-deficient) sites.
 //
+// Range: the sums behind |x|, v^H a and V^H x are taken on x scaled by 2^-e, e the binary
+// exponent of the largest |Re|, |Im| of x when that lies outside [2^-256, 2^257) and 0 inside
+// (each CTA its own e; the partials are brought to the largest e on combination), and the
+// reflector is formed on (alpha, x) scaled by 2^-E, E the larger of that exponent and alpha's
+// (taken the same way).  Inside the range nothing is scaled: the instruction stream is the
+// plain formula's.  Outside it the scalings are exact powers of two, so columns whose norm is
+// near or below sqrt(DBL_MIN) (amplitudes of 1e-150 and smaller occur in the sweeps from
+// product states) get the reflector zlarfg's safe-minimum rescaling gives them instead of an
+// overflow.  Not covered: an unscaled column's products with entries below 2^-766 of another
+// column underflow (LAPACK's normalised v keeps them), i.e. spreads of more than ~1e-230
+// between the columns of one matrix lose those small columns' directions.
+//
 // B200 mapping: one thread-block cluster per matrix, rows split over its C CTAs (32*RPL
 // rows each; the whole matrix lives in distributed shared memory).  Blocked right-looking
 // algorithm with panels of NB columns.  Every exchange between CTAs is a *push*: the
@@ -119,6 +131,82 @@ __device__ __forceinline__ cd sum_ranks(const cd* part, int stride, int C) {
   return v[0];
 }
 
+// The exponent slot of a rank's column message: no nonzero entry below the diagonal.
+constexpr int ESENT = -100000;
+
+// 2^k for -1022 <= k <= 1023, written into the exponent field
+__device__ __forceinline__ double pow2i(int k) { return __hiloint2double((k + 1023) << 20, 0); }
+// 2^k for k <= 0; 0 below the normal range (a contribution 2^-1022 times smaller than the rest)
+__device__ __forceinline__ double pow2neg(int k) { return k >= -1022 ? pow2i(k) : 0.0; }
+// binary exponent (clamped to [-1022, 1022]) of a nonnegative double from its high word;
+// high word 0 (|v| < 2^-1042) is the caller's "zero"
+__device__ __forceinline__ int expo_hi(unsigned hi) {
+  const int b = (int)((hi >> 20) & 0x7ffu);
+  return min(max(b, 1) - 1023, 1022);
+}
+__device__ __forceinline__ cd cscal(cd v, double f) { return cmk(v.x * f, v.y * f); }
+
+// Half-width of the binary-exponent window [2^-SWIN, 2^(SWIN+1)) inside which nothing is scaled.
+constexpr int SWIN = 256;
+constexpr double WHI = 0x1p256, WLO = 0x1p-256;   // 2^SWIN, 2^-SWIN
+static_assert(SWIN == 256, "WHI / WLO follow SWIN");
+
+// A CTA whose partials are those of x 2^-e sends its |x|^2 partial (real) in the imaginary
+// part and a quiet NaN carrying SCODE + e in the real part, so the unscaled combination of the
+// ranks is NaN exactly when some rank scaled.
+constexpr long long SCODE = 4096;
+__device__ __forceinline__ double scale_nan(int e) {
+  return __longlong_as_double(0x7ff8000000000000ll | (unsigned long long)(SCODE + e));
+}
+__device__ __forceinline__ int scale_of_nan(double v) { return (int)((__double_as_longlong(v) & 0xffffll) - SCODE); }
+
+// The reflector when some rank scaled its partials or alpha lies outside the unit range (rare:
+// kept out of line so the common path's instructions stay the plain formula's).  Lane c < pw
+// of warp 0 gets s = its combined partial at the scale 2^-E (lane jl: |x|^2 at 2^-2E), and
+// every lane tau, beta, rs = 1/(alpha - beta) at 2^-E, and fE = 2^-E.
+__device__ __noinline__ void reflector_scaled(const cd* rb, int RS, int C, int lane, int jl, int pw, cd alpha,
+                                              cd& s, cd& tau, cd& beta, cd& rs, double& fE) {
+  int e[CMAX];
+  int ex = ESENT;
+#pragma unroll
+  for (int q = 0; q < CMAX; ++q) {
+    e[q] = ESENT;
+    if (q < C) {
+      const cd pq = rb[q * RS + jl];
+      e[q] = pq.x != pq.x ? scale_of_nan(pq.x) : (pq.x != 0.0 ? 0 : ESENT);
+    }
+    ex = max(ex, e[q]);
+  }
+  cd v = cmk(0.0, 0.0);
+  if (lane < pw) {
+    const int mult = lane == jl ? 2 : 1;
+#pragma unroll
+    for (int q = 0; q < CMAX; ++q) {
+      if (q >= C || e[q] == ESENT) continue;
+      cd pq = rb[q * RS + lane];
+      if (lane == jl) pq = cmk(pq.x != pq.x ? pq.y : pq.x, 0.0);
+      v = cadd(v, cscal(pq, pow2neg(mult * (e[q] - ex))));
+    }
+  }
+  const double xn2x = __shfl_sync(0xffffffffu, v.x, jl);   // |x|^2 2^-2ex
+  const unsigned ha = (unsigned)__double2hiint(fmax(fabs(alpha.x), fabs(alpha.y)));
+  int ea = expo_hi(ha);
+  ea = (ha == 0u) ? ESENT : (ea >= -SWIN && ea <= SWIN ? 0 : ea);
+  const int E = max(ex, ea);   // not both ESENT: x == 0 with real alpha never gets here
+  fE = pow2i(-E);
+  const cd as = cscal(alpha, fE);
+  const double xn2 = (ex == ESENT) ? 0.0 : xn2x * pow2neg(2 * (ex - E));
+  const double nrm = sqrt(as.x * as.x + as.y * as.y + xn2);
+  const double b = -copysign(nrm, alpha.x);
+  const double dr = as.x - b;
+  const double ib = 1.0 / b;
+  const double id = 1.0 / (dr * dr + as.y * as.y);
+  tau = cmk((b - as.x) * ib, -as.y * ib);
+  beta = cmk(b * pow2i(E), 0.0);
+  rs = cmk(dr * id, -as.y * id);
+  s = (ex == ESENT) ? cmk(0.0, 0.0) : cscal(v, pow2neg(ex - E));
+}
+
 __device__ __forceinline__ cd shfl(cd v, int src) {
   return cmk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
@@ -211,7 +299,7 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
   cd* w2s = sm + P.o_w2s;
   cd* rag = sm + P.o_rag;
   cd* Tall = sm + P.o_T;
-  cd* bcs = sm + P.o_bc;        // tau, beta, scale of the current column
+  cd* bcs = sm + P.o_bc;        // tau, beta, 1/(alpha - beta) at scale 2^-E, and 2^-E of the current column
   cd* bcw = bcs + 4;            // w_c of the current column
   cd* tst = sm + P.o_tst;       // tst[jl*NB + c] = t_c (c < jl), tst[jl*NB + jl] = tau_jl
   uint64_t* mb = reinterpret_cast<uint64_t*>(smem_raw + P.o_mbar);
@@ -244,7 +332,8 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
     const int pw = min(NB, n - p0);
     for (int jl = 0; jl < pw; ++jl) {
       const int j = p0 + jl;
-      cd* rb = rcol + sp * (C * 2 * NB);
+      constexpr int RS = 2 * NB;   // per rank: NB sums, NB owner-row values
+      cd* rb = rcol + sp * (C * RS);
       const uint32_t mbc = mbs[MB_COL0 + sp];
       const int owner = j / ROWS;
       // -- phase A: partial sums over this CTA's rows g > j, pushed to every CTA
@@ -258,36 +347,66 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
         static_assert(NB <= 2 * NW, "at most two panel columns per warp");
         const int c0 = warp, c1 = warp + NW;
         cd a0 = cmk(0.0, 0.0), a1 = cmk(0.0, 0.0);
+        double mx = 0.0;   // largest |Re|, |Im| of x over this CTA's rows (every warp finds the same)
 #pragma unroll
-        for (int q = 0; q < RPL; ++q) {
-          const int r = lane + 32 * q;
-          if (c0 < pw) {
-            const cd a = S[(p0 + c0) * ldS + r];
-            if (c0 >= jl) cfma_cj(a0, x[q], a);   // conj(x) a  (c == jl: |x|^2)
-            else          cfma_cj(a0, a, x[q]);   // conj(a) x  (V^H x for the T column)
+        for (int q = 0; q < RPL; ++q) mx = fmax(mx, fmax(fabs(x[q].x), fabs(x[q].y)));
+        const unsigned hb = __reduce_max_sync(0xffffffffu, (unsigned)__double2hiint(mx));
+        auto partials = [&](const cd (&xv)[RPL]) {
+#pragma unroll
+          for (int q = 0; q < RPL; ++q) {
+            const int r = lane + 32 * q;
+            if (c0 < pw) {
+              const cd a = S[(p0 + c0) * ldS + r];
+              if (c0 == jl)     cfma_cj(a0, xv[q], xv[q]);   // |x|^2
+              else if (c0 > jl) cfma_cj(a0, xv[q], a);       // conj(x) a
+              else              cfma_cj(a0, a, xv[q]);       // conj(a) x  (V^H x for the T column)
+            }
+            if (c1 < pw) {
+              const cd a = S[(p0 + c1) * ldS + r];
+              if (c1 == jl)     cfma_cj(a1, xv[q], xv[q]);
+              else if (c1 > jl) cfma_cj(a1, xv[q], a);
+              else              cfma_cj(a1, a, xv[q]);
+            }
           }
-          if (c1 < pw) {
-            const cd a = S[(p0 + c1) * ldS + r];
-            if (c1 >= jl) cfma_cj(a1, x[q], a);
-            else          cfma_cj(a1, a, x[q]);
+        };
+        auto reduce = [&]() {
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            a0.x += __shfl_xor_sync(0xffffffffu, a0.x, off);
+            a0.y += __shfl_xor_sync(0xffffffffu, a0.y, off);
+            a1.x += __shfl_xor_sync(0xffffffffu, a1.x, off);
+            a1.y += __shfl_xor_sync(0xffffffffu, a1.y, off);
+          }
+        };
+        partials(x);
+        // this CTA's scale 2^-e: e = 0 inside the window (the partials above stand), else mx's
+        // binary exponent, and the partials are those of x 2^-e (ESENT: x == 0, or below 2^-1042)
+        const int ee = expo_hi(hb);
+        const int e_loc = (hb == 0u) ? ESENT : (ee >= -SWIN && ee <= SWIN ? 0 : ee);
+        if (e_loc != 0 && e_loc != ESENT) {
+          {
+            const double f = pow2i(-e_loc);
+            cd xs[RPL];
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) xs[q] = cscal(x[q], f);
+            a0 = a1 = cmk(0.0, 0.0);
+            partials(xs);
           }
         }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          a0.x += __shfl_xor_sync(0xffffffffu, a0.x, off);
-          a0.y += __shfl_xor_sync(0xffffffffu, a0.y, off);
-          a1.x += __shfl_xor_sync(0xffffffffu, a1.x, off);
-          a1.y += __shfl_xor_sync(0xffffffffu, a1.y, off);
-        }
+        reduce();
         if (lane < C) {
           const uint32_t rm = mapa(mbc, lane);
-          if (c0 < pw) st_async(mapa(su32(&rb[crank * 2 * NB + c0]), lane), a0, rm);
-          if (c1 < pw) st_async(mapa(su32(&rb[crank * 2 * NB + c1]), lane), a1, rm);
+          if (e_loc != 0 && e_loc != ESENT) {
+            if (c0 == jl) a0 = cmk(scale_nan(e_loc), a0.x);
+            if (c1 == jl) a1 = cmk(scale_nan(e_loc), a1.x);
+          }
+          if (c0 < pw) st_async(mapa(su32(&rb[crank * RS + c0]), lane), a0, rm);
+          if (c1 < pw) st_async(mapa(su32(&rb[crank * RS + c1]), lane), a1, rm);
         }
       }
       if (crank == owner && warp == NW - 1 && lane < pw) {
         const cd v = S[(p0 + lane) * ldS + (j - row0)];
-        for (int q = 0; q < C; ++q) st_async(mapa(su32(&rb[crank * 2 * NB + NB + lane]), q), v, mapa(mbc, q));
+        for (int q = 0; q < C; ++q) st_async(mapa(su32(&rb[crank * RS + NB + lane]), q), v, mapa(mbc, q));
       }
       if (tid == 0) mbar_expect(mbc, (uint32_t)((C + 1) * pw * sizeof(cd)));
       cta_wait(mbc, ph[MB_COL0 + sp], failed, err);
@@ -297,16 +416,18 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
       if (warp == 0) {
         cd s = cmk(0.0, 0.0), rj = cmk(0.0, 0.0);
         if (lane < pw) {
-          s = sum_ranks(rb + lane, 2 * NB, C);
-          rj = rb[owner * 2 * NB + NB + lane];
+          s = sum_ranks(rb + lane, RS, C);
+          rj = rb[owner * RS + NB + lane];
         }
         const cd alpha = shfl(rj, jl);
-        const double xn2 = __shfl_sync(0xffffffffu, s.x, jl);
-        cd tau, beta, scale;
-        if (xn2 == 0.0 && alpha.y == 0.0) {
-          tau = cmk(0.0, 0.0); beta = alpha; scale = cmk(1.0, 0.0);
-        } else {
-          // tau = (beta - alpha)/beta and scale = 1/(alpha - beta) from two independent
+        const double xn2 = __shfl_sync(0xffffffffu, s.x, jl);   // NaN: some rank scaled its partials
+        const double am = fabs(alpha.x) + fabs(alpha.y);   // alpha's window: (2^-SWIN, 2^SWIN)
+        cd tau, beta, rs;
+        double fE = 1.0;
+        if (xn2 == 0.0 && alpha.y == 0.0) {   // x == 0 (an unscaled nonzero x has |x|^2 >= 2^-2SWIN)
+          tau = cmk(0.0, 0.0); beta = alpha; rs = cmk(1.0, 0.0);
+        } else if (xn2 >= 0.0 && am < WHI && (xn2 > 0.0 || am > WLO)) {
+          // tau = (beta - alpha)/beta and rs = 1/(alpha - beta) from two independent
           // reciprocals, 1/beta and 1/|alpha - beta|^2 (Re(alpha) - beta has no cancellation:
           // beta carries the opposite sign of Re(alpha))
           const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
@@ -316,20 +437,24 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
           const double id = 1.0 / (dr * dr + alpha.y * alpha.y);
           tau = cmk((b - alpha.x) * ib, -alpha.y * ib);
           beta = cmk(b, 0.0);
-          scale = cmk(dr * id, -alpha.y * id);
+          rs = cmk(dr * id, -alpha.y * id);
+        } else {
+          reflector_scaled(rb, RS, C, lane, jl, pw, alpha, s, tau, beta, rs, fE);
         }
-        if (lane > jl && lane < pw) bcw[lane] = cadd(rj, cmul(cconj(scale), s));
-        else if (lane < jl) tst[jl * NB + lane] = cadd(cconj(rj), cmul(scale, s));
-        if (lane == 0) { bcs[0] = tau; bcs[1] = beta; bcs[2] = scale; tst[jl * NB + jl] = tau; }
+        // w_c = a_c[j] + conj(rs) (x 2^-E)^H a_c and t_c = conj(V[j, c]) + rs V[:, c]^H (x 2^-E)
+        if (lane > jl && lane < pw) bcw[lane] = cadd(rj, cmul(cconj(rs), s));
+        else if (lane < jl) tst[jl * NB + lane] = cadd(cconj(rj), cmul(rs, s));
+        if (lane == 0) { bcs[0] = tau; bcs[1] = beta; bcs[2] = rs; bcs[3] = cmk(fE, 0.0); tst[jl * NB + jl] = tau; }
       }
       __syncthreads();
-      const cd tau = bcs[0], beta = bcs[1], scale = bcs[2];
+      const cd tau = bcs[0], beta = bcs[1], rs = bcs[2];
+      const double fE = bcs[3].x;
       if ((tau.x != 0.0) || (tau.y != 0.0)) {
         cd vr[RPL];
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {
           int g = row0 + lane + 32 * q;
-          vr[q] = (g == j) ? cmk(1.0, 0.0) : cmul(scale, x[q]);   // x is 0 above j and in padding
+          vr[q] = (g == j) ? cmk(1.0, 0.0) : cmul(rs, fE == 1.0 ? x[q] : cscal(x[q], fE));   // x is 0 above j and in padding
         }
         const cd ctau = cconj(tau);
         if (warp == (jl % NW)) {
@@ -485,7 +610,7 @@ size_t layout(QrParams& P, int n, int C, int rows, int nb) {
   P.o_w2s = o;   o += nb * P.ksmax;
   P.o_rag = o;   o += nb * n;
   P.o_T = o;     o += nb * nb;
-  P.o_bc = o;    o += 4 + nb;        // tau, beta, scale, pad; w[nb]
+  P.o_bc = o;    o += 4 + nb;        // tau, beta, rs, 2^-E; w[nb]
   P.o_tst = o;   o += nb * nb;       // t vectors (and tau) of the panel's columns
   P.o_mbar = o * (int)sizeof(cd);
   return (size_t)P.o_mbar + MB_COUNT * sizeof(uint64_t);

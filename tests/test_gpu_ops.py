@@ -65,6 +65,24 @@ def test_qr_mixed_exact_zero_columns(gpu_ctx):
     assert np.abs(Q.conj().T @ Q - np.eye(24)).max() < 1e-12
 
 
+@pytest.mark.parametrize("m,n", [(64, 16), (64, 32), (200, 48), (512, 128), (1024, 300)])
+def test_qr_tiny_columns_match_lapack(gpu_ctx, m, n):
+    """Columns scaled down to 1e-240 (the sweeps from product states produce amplitudes of
+    1e-150 and below): Householder QR is invariant under positive column scaling, Q(X D) = Q(X)
+    and R(X D) = R(X) D, which LAPACK keeps through zlarfg's rescaling; so must the GPU."""
+    rng = np.random.default_rng(m * 7 + n)
+    X = crand(rng, m, n)
+    e = rng.choice([0, 40, 80, 150, 154, 158, 162, 200, 240], size=n)
+    D = 10.0 ** (-e.astype(float))
+    q_ref, r_ref = R.julia_qr(X)
+    dX, dQ, dR = to_dev(X * D), empty_dev((m, n)), empty_dev((n, n))
+    _call(gpu_ctx, "mpsb_op_qr", _p(dX), _p(dQ), _p(dR), m, n)
+    Q, Rr = from_dev(dQ, (m, n)), from_dev(dR, (n, n))
+    assert np.isfinite(Q).all() and np.isfinite(Rr).all()
+    assert np.abs(Q - q_ref).max() < 1e-11
+    assert np.abs(Rr / D - r_ref).max() < 1e-11 * np.abs(r_ref).max()
+
+
 @pytest.mark.parametrize("m,n", [(2048, 512), (1024, 300), (640, 40)])
 def test_qr_blocked_path_matches_lapack(gpu_ctx, m, n):
     """Shapes beyond one cluster's shared memory (2048 x 512 is the interior site of a
