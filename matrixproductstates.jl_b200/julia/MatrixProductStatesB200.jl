@@ -172,4 +172,47 @@ function scal_prod_no_conj(ctx::Ctx, A::DMPS, B::DMPS)
     return complex(out[1], out[2])
 end
 
+# Wrap a handle the library created (its dims read back through mpsb_mps_info)
+function wrap_new_mps(h::Ptr{Cvoid})
+    na, d = Ref{Cint}(0), Ref{Cint}(0)
+    check(ccall((:mpsb_mps_info, LIB), Cint, (Ptr{Cvoid}, Ref{Cint}, Ref{Cint}, Ptr{Int64}), h, na, d, C_NULL),
+          :mpsb_mps_info)
+    dims = zeros(Int64, na[] + 1)
+    check(ccall((:mpsb_mps_info, LIB), Cint, (Ptr{Cvoid}, Ref{Cint}, Ref{Cint}, Ptr{Int64}), h, na, d, dims),
+          :mpsb_mps_info)
+    m = DMPS(h, dims, Int(d[]))
+    finalizer(x -> ccall((:mpsb_mps_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), m)
+    return m
+end
+
+# compressionSVD!(mps, dmax, tol)   src/compression.jl:1280-1312
+# Returns (new MPS with the truncated bond dims, err_glob, err_trim, ent_ent); the reference
+# resizes `mps` in place, here the result is a new handle.
+function compressionSVD!(ctx::Ctx, A::DMPS, dmax::Integer, tol::Real)
+    na = length(A.dims) - 1
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    err_glob = Ref{Cdouble}(0)
+    err_trim, ent = zeros(Cdouble, na), zeros(Cdouble, na)
+    check(ccall((:mpsb_compression_svd, LIB), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cdouble, Ptr{Ptr{Cvoid}}, Ref{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+                ctx.h, A.h, dmax, tol, out, err_glob, err_trim, ent), :mpsb_compression_svd)
+    return wrap_new_mps(out[]), err_glob[], err_trim, ent
+end
+
+# compress_var_apply_H_two_site(Ain, A, H, maxsweeps, svd_tol, dims, dlim)   src/compression.jl:355-411
+# Returns the compressed MPS (new handle; its `dims` are the reference's updated dims).
+function compress_var_apply_H_two_site(ctx::Ctx, Ain::DMPS, A::DMPS, H::DMPO, maxsweeps::Integer,
+                                       svd_tol::Real, dlim::Integer)
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:mpsb_compress_var_apply_H_two_site, LIB), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cdouble, Cint, Ptr{Ptr{Cvoid}}),
+                ctx.h, Ain.h, A.h, H.h, maxsweeps, svd_tol, dlim, out), :mpsb_compress_var_apply_H_two_site)
+    return wrap_new_mps(out[])
+end
+
+# Two-lane RK4 step on (1, default) or off (0); no reference counterpart (results are identical)
+set_pipeline!(ctx::Ctx, enable::Bool) =
+    check(ccall((:mpsb_ctx_set_pipeline, LIB), Cint, (Ptr{Cvoid}, Cint), ctx.h, enable ? 1 : 0),
+          :mpsb_ctx_set_pipeline)
+
 end # module

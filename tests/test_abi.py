@@ -71,3 +71,11 @@ def test_dims_rule_host_logic():
     from mpsb200.core import _dims_rule
     for (na, dmax, d) in [(20, 32, 2), (40, 128, 4), (64, 256, 2), (3, 5, 3)]:
         assert _dims_rule(na, dmax, d) == R.dims_rule(na, dmax, d)
+
+
+def test_julia_shim_binds_only_declared_symbols():
+    """Every ccall of the Julia shim names an entry point that include/mpsb.h declares."""
+    jl = open(os.path.join(PKG_DIR, "julia", "MatrixProductStatesB200.jl")).read()
+    called = set(re.findall(r"ccall\(\(:(mpsb_[A-Za-z0-9_]+),", jl))
+    assert "mpsb_rk4stp_apply_H_half" in called
+    assert called <= set(declared_symbols()), sorted(called - set(declared_symbols()))
