@@ -163,9 +163,14 @@ __device__ __forceinline__ int scale_of_nan(double v) { return (int)((__double_a
 // The reflector when some rank scaled its partials or alpha lies outside the unit range (rare:
 // kept out of line so the common path's instructions stay the plain formula's).  Lane c < pw
 // of warp 0 gets s = its combined partial at the scale 2^-E (lane jl: |x|^2 at 2^-2E), and
-// every lane tau, beta, rs = 1/(alpha - beta) at 2^-E, and fE = 2^-E.
-__device__ __noinline__ void reflector_scaled(const cd* rb, int RS, int C, int lane, int jl, int pw, cd alpha,
-                                              cd& s, cd& tau, cd& beta, cd& rs, double& fE) {
+// every lane tau, beta, rs = 1/(alpha - beta) at 2^-E, and fE = 2^-E.  Returned by value, so
+// the caller's variables stay in registers on the common path.
+struct Reflector {
+  cd s, tau, beta, rs;
+  double fE;
+};
+__device__ __noinline__ Reflector reflector_scaled(const cd* rb, int RS, int C, int lane, int jl, int pw, cd alpha) {
+  Reflector o;
   int e[CMAX];
   int ex = ESENT;
 #pragma unroll
@@ -193,18 +198,19 @@ __device__ __noinline__ void reflector_scaled(const cd* rb, int RS, int C, int l
   int ea = expo_hi(ha);
   ea = (ha == 0u) ? ESENT : (ea >= -SWIN && ea <= SWIN ? 0 : ea);
   const int E = max(ex, ea);   // not both ESENT: x == 0 with real alpha never gets here
-  fE = pow2i(-E);
-  const cd as = cscal(alpha, fE);
+  o.fE = pow2i(-E);
+  const cd as = cscal(alpha, o.fE);
   const double xn2 = (ex == ESENT) ? 0.0 : xn2x * pow2neg(2 * (ex - E));
   const double nrm = sqrt(as.x * as.x + as.y * as.y + xn2);
   const double b = -copysign(nrm, alpha.x);
   const double dr = as.x - b;
   const double ib = 1.0 / b;
   const double id = 1.0 / (dr * dr + as.y * as.y);
-  tau = cmk((b - as.x) * ib, -as.y * ib);
-  beta = cmk(b * pow2i(E), 0.0);
-  rs = cmk(dr * id, -as.y * id);
-  s = (ex == ESENT) ? cmk(0.0, 0.0) : cscal(v, pow2neg(ex - E));
+  o.tau = cmk((b - as.x) * ib, -as.y * ib);
+  o.beta = cmk(b * pow2i(E), 0.0);
+  o.rs = cmk(dr * id, -as.y * id);
+  o.s = (ex == ESENT) ? cmk(0.0, 0.0) : cscal(v, pow2neg(ex - E));
+  return o;
 }
 
 __device__ __forceinline__ cd shfl(cd v, int src) {
@@ -379,21 +385,20 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
           }
         };
         partials(x);
-        // this CTA's scale 2^-e: e = 0 inside the window (the partials above stand), else mx's
-        // binary exponent, and the partials are those of x 2^-e (ESENT: x == 0, or below 2^-1042)
+        reduce();
+        // this CTA's scale 2^-e: e = 0 inside the window (the sums above stand), else mx's
+        // binary exponent, and the sums are redone on x 2^-e (ESENT: x == 0, or below 2^-1042)
         const int ee = expo_hi(hb);
         const int e_loc = (hb == 0u) ? ESENT : (ee >= -SWIN && ee <= SWIN ? 0 : ee);
         if (e_loc != 0 && e_loc != ESENT) {
-          {
-            const double f = pow2i(-e_loc);
-            cd xs[RPL];
+          const double f = pow2i(-e_loc);
+          cd xs[RPL];
 #pragma unroll
-            for (int q = 0; q < RPL; ++q) xs[q] = cscal(x[q], f);
-            a0 = a1 = cmk(0.0, 0.0);
-            partials(xs);
-          }
+          for (int q = 0; q < RPL; ++q) xs[q] = cscal(x[q], f);
+          a0 = a1 = cmk(0.0, 0.0);
+          partials(xs);
+          reduce();
         }
-        reduce();
         if (lane < C) {
           const uint32_t rm = mapa(mbc, lane);
           if (e_loc != 0 && e_loc != ESENT) {
@@ -439,7 +444,8 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
           beta = cmk(b, 0.0);
           rs = cmk(dr * id, -alpha.y * id);
         } else {
-          reflector_scaled(rb, RS, C, lane, jl, pw, alpha, s, tau, beta, rs, fE);
+          const Reflector o = reflector_scaled(rb, RS, C, lane, jl, pw, alpha);
+          s = o.s; tau = o.tau; beta = o.beta; rs = o.rs; fE = o.fE;
         }
         // w_c = a_c[j] + conj(rs) (x 2^-E)^H a_c and t_c = conj(V[j, c]) + rs V[:, c]^H (x 2^-E)
         if (lane > jl && lane < pw) bcw[lane] = cadd(rj, cmul(cconj(rs), s));
