@@ -236,6 +236,25 @@ int mpsb_compress_var_apply_H_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const
                                        const mpsb_mpo* H, int maxsweeps, double svd_tol, int dlim,
                                        mpsb_mps** out);
 
+/* compress_sum_var_apply_H_two_site(Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim)
+ *   src/compression.jl:1072-1157 (half = 0), its _left form :1159-1215 (half = 1: one R->L
+ *   sweep, first site U diag(S)) and _right form :1218-1276 (half = 2: one L->R sweep from the
+ *   right environments of a right-canonical Ain, coefficients on the left boundary; the
+ *   operator term's is stored conjugated there, since that environment is contracted
+ *   conjugated, so the result is the stated sum also for complex coefficients);
+ * compress_sum_var_two_site(Ain, coef, A, maxsweeps, svd_tol, dims, dlim)  :574-648 when H is NULL.
+ * Two-site variational compression of sum_l coef[l] A[l], the last term through H when H is
+ * given; coef is numv interleaved complex (numv plain terms at most 8 besides the H term); every
+ * A[l] has the bond dims of A[numv-1]; Ain is the left-canonical guess (right-canonical for
+ * half = 2).  Bond dims adapt (<= dlim): the result is a new handle *out.  As in
+ * mpsb_compress_var_apply_H_two_site the undefined `svdecon` is the thin SVD and the pair
+ * contractions use the environments as the single-site path does (the reference's
+ * A_prod_LR_two_site, src/MatrixProductStates.jl:288-292, contracts the stored left
+ * environment on its A0 index, i.e. transposed). */
+int mpsb_compress_sum_var_apply_H_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const double* coef, int numv,
+                                           const mpsb_mps* const* A, const mpsb_mpo* H, int maxsweeps,
+                                           double svd_tol, int dlim, int half, mpsb_mps** out);
+
 /* svd(M) as compressionSVD! calls it (src/compression.jl:1296): thin SVD X = U diag(S) V^H of a
  * device m x n column-major matrix, k = min(m, n); U (m x k) and V (n x k) device, S (k) host,
  * singular values descending.  One-sided Jacobi (relative accuracy); phases of the singular

@@ -692,6 +692,26 @@ int mpsb_compress_var_apply_H_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const
   return sync(ctx);
 }
 
+int mpsb_compress_sum_var_apply_H_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const double* coef, int numv,
+                                           const mpsb_mps* const* A, const mpsb_mpo* H, int maxsweeps,
+                                           double svd_tol, int dlim, int half, mpsb_mps** out) {
+  MPSB_TRY(bind(ctx));
+  if (!out || !coef || !A || numv < 1 || numv > 9) return MPSB_ERR_INVALID_ARG;
+  std::vector<cd> c(numv);
+  for (int l = 0; l < numv; ++l) c[l] = cmk(coef[2 * l], coef[2 * l + 1]);
+  std::vector<int64_t> dims, offs;
+  cd* sites = nullptr;
+  MPSB_TRY(compress_two_site_sum(ctx, Ain, numv, c.data(), A, H, maxsweeps, svd_tol, dlim, half, dims, offs, &sites));
+  const mpsb_mps* T = A[numv - 1];
+  mpsb_mps* R = nullptr;
+  MPSB_TRY(mpsb_mps_create(ctx, T->na, T->d, dims.data(), &R));
+  for (int k = 0; k < T->na; ++k)
+    MPSB_CUDA_TRY(cudaMemcpyAsync(R->site(k), sites + offs[k], R->site_elems(k) * sizeof(cd), cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+  *out = R;
+  return sync(ctx);
+}
+
 int mpsb_op_svd(mpsb_ctx* ctx, const void* X, void* U, double* S, void* V, int m, int n) {
   MPSB_TRY(bind(ctx));
   if (!X || !U || !S || !V || m < 1 || n < 1) return MPSB_ERR_DIMENSION;

@@ -125,6 +125,9 @@ int compression_svd(mpsb_ctx* ctx, const mpsb_mps* in, int dmax, double tol, std
 int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, const mpsb_mpo* H, int maxsweeps,
                       double svd_tol, int dlim, std::vector<int64_t>& dims_out, std::vector<int64_t>& offs,
                       cd** sites);
+int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd* coef, const mpsb_mps* const* Av,
+                          const mpsb_mpo* H, int maxsweeps, double svd_tol, int dlim, int mode,
+                          std::vector<int64_t>& dims_out, std::vector<int64_t>& offs, cd** sites);
 int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, const mpsb_mpo* H3,
              mpsb_mps* psi0, mpsb_mps* psi, mpsb_mps* psi1, mpsb_mps* psi2, mpsb_mps* psi3, mpsb_env* env1,
              mpsb_env* env2, mpsb_env* env3, mpsb_env* envop);

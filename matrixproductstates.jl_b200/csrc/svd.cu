@@ -352,18 +352,36 @@ int truncation_rule(const std::vector<double>& S, int k, double tol, int dlim) {
 
 }  // namespace
 
-// compress_var_apply_H_two_site (src/compression.jl:355-411): maxsweeps sweep pairs of the
-// two-site variational compression of H A with guess Ain; each pair's effective tensor
-// av[a0,s1,s2,b0] = sum L[a,w,a0]* A1[a,t1,c] O1[w,s1,v,t1] A2[c,t2,b] O2[v,s2,u,t2] R[b,u,b0]
-// (the left environment conjugated as every single-site contraction uses it) is split by a
-// thin SVD, truncated by the compressionSVD! rule (svd_tol, dlim), the bond updated.  Bond
-// dims change; the result lands in context scratch (site k at offs[k]) with dims_out.
-int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, const mpsb_mpo* H, int maxsweeps,
-                      double svd_tol, int dlim, std::vector<int64_t>& dims_out, std::vector<int64_t>& offs,
-                      cd** sites) {
-  if (!ctx || !Ain || !A || !H || maxsweeps < 1 || dlim < 1 || !(svd_tol >= 0)) return MPSB_ERR_INVALID_ARG;
+// compress_sum_var_apply_H_two_site (src/compression.jl:1072-1157) and its relatives: the
+// two-site variational compression of  sum_l coef[l] A[l]  (+ coef[numv-1] H A[numv-1] when H
+// is given) with guess Ain.  Each pair's effective tensor is
+//   av[a0,s1,s2,b0] = sum_l FL_l[a0,a] A_l1[a,s1,c] A_l2[c,s2,b] FR_l[b,b0]
+//                   + sum conj(L[a,w,a0]) A1[a,t1,c] O1[w,s1,v,t1] A2[c,t2,b] O2[v,s2,u,t2] R[b,u,b0]
+// (the 2-index left environment contracted on its A index and the 3-index one conjugated,
+// as every single-site contraction uses them), split by a thin SVD and truncated by the
+// compressionSVD! rule (svd_tol, dlim).  mode 0: maxsweeps sweep pairs (R->L then L->R, the
+// coefficients on the right boundary); mode 1: one R->L half sweep (the _left form, last site
+// U diag(S)); mode 2: one L->R half sweep from right environments of a right-canonical guess
+// (the _right form, coefficients on the left boundary, last site diag(S) V').  Bond dims
+// change; the result lands in context scratch (site k at offs[k]) with dims_out.  Every A[l]
+// has the bond dims of A[numv-1].
+int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd* coef, const mpsb_mps* const* Av,
+                          const mpsb_mpo* H, int maxsweeps, double svd_tol, int dlim, int mode,
+                          std::vector<int64_t>& dims_out, std::vector<int64_t>& offs, cd** sites) {
+  if (!ctx || !Ain || numv < 1 || !coef || !Av || maxsweeps < 1 || dlim < 1 || !(svd_tol >= 0) || mode < 0 ||
+      mode > 2)
+    return MPSB_ERR_INVALID_ARG;
+  const bool hasH = H != nullptr;
+  const int np = hasH ? numv - 1 : numv;   // plain terms
+  if (np > 8) return MPSB_ERR_UNSUPPORTED;
+  for (int l = 0; l < numv; ++l)
+    if (!Av[l]) return MPSB_ERR_INVALID_ARG;
+  const mpsb_mps* A = Av[numv - 1];
   const int na = A->na, d = A->d;
-  if (Ain->na != na || Ain->d != d || H->na != na || H->d != d || na < 2) return MPSB_ERR_DIMENSION;
+  if (Ain->na != na || Ain->d != d || na < 2) return MPSB_ERR_DIMENSION;
+  if (hasH && (H->na != na || H->d != d)) return MPSB_ERR_DIMENSION;
+  for (int l = 0; l < numv; ++l)
+    if (Av[l]->na != na || Av[l]->d != d || Av[l]->dims != A->dims) return MPSB_ERR_DIMENSION;
   cudaStream_t st = ctx->stream;
   std::vector<int64_t> dims = Ain->dims, cap(na + 1);
   for (int k = 0; k <= na; ++k) {   // capacity of bond k: the dims rule bound with dlim
@@ -373,11 +391,12 @@ int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, con
     cap[k] = std::max<int64_t>(dims[k], std::min(c, std::min(pl, pr)));
   }
   auto DA = [&](int k) { return (int)A->dims[k]; };
-  auto W = [&](int k) { return (int)H->w[k]; };
-  // scratch: A0 sites at capacity, FL and FR stacks, the pair tensors and the SVD factors
+  auto W = [&](int k) { return hasH ? (int)H->w[k] : 1; };
+  // scratch: A0 sites at capacity, the FL / FR stacks (3-index for the H term, 2-index for each
+  // plain term), two contraction buffers, the pair tensor and the SVD factors
   offs.assign(na, 0);
-  int64_t tot = 0, envtot = 0, pairmax = 1, aor = 1;
-  std::vector<int64_t> eoff(na + 1);
+  int64_t tot = 0, envtot = 0, env2tot = 0, pairmax = 1, aor = 1;
+  std::vector<int64_t> eoff(na + 1), e2off(na + 1);
   for (int k = 0; k < na; ++k) {
     offs[k] = tot;
     tot += cap[k] * d * cap[k + 1];
@@ -385,6 +404,8 @@ int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, con
   for (int k = 0; k <= na; ++k) {
     eoff[k] = envtot;
     envtot += (int64_t)DA(k) * W(k) * cap[k];
+    e2off[k] = env2tot;
+    env2tot += (int64_t)DA(k) * cap[k];
   }
   for (int k = 0; k + 1 < na; ++k) {
     pairmax = std::max<int64_t>(pairmax, cap[k] * d * d * cap[k + 2]);
@@ -395,13 +416,15 @@ int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, con
     aor = std::max<int64_t>(aor, (int64_t)DA(k) * W(k) * d * cap[k + 1]);
     aor = std::max<int64_t>(aor, (int64_t)cap[k] * d * DA(k + 1) * W(k + 1));
   }
-  const size_t need = (size_t)tot + 2 * envtot + 2 * aor + 3 * pairmax + pairmax / 2 + 64;
+  const size_t need = (size_t)tot + 2 * (hasH ? envtot : 0) + 2 * (size_t)np * env2tot + 2 * aor + 3 * pairmax +
+                      pairmax / 2 + 64;
   cd* base = nullptr;
   MPSB_TRY(ensure_slot(ctx, SLOT_MISC, need * sizeof(cd), &base));
   cd* A0 = base;
   cd* FLb = A0 + tot;
-  cd* FRb = FLb + envtot;
-  cd* X = FRb + envtot;
+  cd* FRb = FLb + (hasH ? envtot : 0);
+  cd* F2b = FRb + (hasH ? envtot : 0);   // [np][2][env2tot]: FL_l then FR_l
+  cd* X = F2b + 2 * (size_t)np * env2tot;
   cd* Y = X + aor;
   cd* av = Y + aor;
   cd* U = av + pairmax;
@@ -409,27 +432,68 @@ int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, con
   double* dS = reinterpret_cast<double*>(V + pairmax);
   auto FL = [&](int k) { return FLb + eoff[k]; };
   auto FR = [&](int k) { return FRb + eoff[k]; };
+  auto FL2 = [&](int l, int k) { return F2b + (2 * (int64_t)l) * env2tot + e2off[k]; };
+  auto FR2 = [&](int l, int k) { return F2b + (2 * (int64_t)l + 1) * env2tot + e2off[k]; };
   auto site0 = [&](int k) { return A0 + offs[k]; };
-  // A0 starts as the guess (dims of Ain)
-  for (int k = 0; k < na; ++k)
+  const cd ONE_ = cmk(1.0, 0.0), ZERO_ = cmk(0.0, 0.0);
+  for (int k = 0; k < na; ++k)   // A0 starts as the guess (dims of Ain)
     MPSB_CUDA_TRY(cudaMemcpyAsync(site0(k), Ain->site(k), Ain->site_elems(k) * sizeof(cd), cudaMemcpyDeviceToDevice, st));
-  const cd ONE_ = cmk(1.0, 0.0);
-  MPSB_TRY(set_boundary(ctx, FL(0), ONE_));
-  for (int k = 0; k < na - 2; ++k) {   // FL[k+1] = update_le(Ain[k], H[k], A[k], FL[k])
-    MPSB_TRY(op_prod_AOL(ctx, A->site(k), H->site(k), FL(k), Y, DA(k), d, DA(k + 1), W(k), W(k + 1), (int)dims[k]));
-    MPSB_TRY(op_update_le(ctx, site0(k), Y, FL(k + 1), (int)dims[k], d, DA(k + 1), W(k + 1), (int)dims[k + 1]));
+
+  // environment updates from site k of A0 (bond dims a0 -> a1 of A0)
+  auto left_update = [&](int k, int a0, int a1) -> int {   // FL[k+1] from FL[k]
+    for (int l = 0; l < np; ++l) {
+      MPSB_TRY(op_L2_A3(ctx, FL2(l, k), Av[l]->site(k), X, a0, DA(k), d * DA(k + 1), ONE_, ZERO_, false));
+      MPSB_TRY(op_update_lenv(ctx, site0(k), X, FL2(l, k + 1), a0 * d, a1, DA(k + 1), true));
+    }
+    if (hasH) {
+      MPSB_TRY(op_prod_AOL(ctx, A->site(k), H->site(k), FL(k), Y, DA(k), d, DA(k + 1), W(k), W(k + 1), a0));
+      MPSB_TRY(op_update_le(ctx, site0(k), Y, FL(k + 1), a0, d, DA(k + 1), W(k + 1), a1));
+    }
+    return MPSB_OK;
+  };
+  auto right_update = [&](int k, int a0, int a1) -> int {   // FR[k] from FR[k+1]
+    for (int l = 0; l < np; ++l) {
+      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(k), FR2(l, k + 1), X, DA(k) * d, DA(k + 1), a1, ONE_, ZERO_));
+      MPSB_TRY(op_update_renv(ctx, site0(k), X, FR2(l, k), DA(k), a0, d * a1));
+    }
+    if (hasH) {
+      MPSB_TRY(op_prod_AOR(ctx, A->site(k), H->site(k), FR(k + 1), X, DA(k), d, DA(k + 1), W(k), W(k + 1), a1));
+      MPSB_TRY(op_update_re(ctx, site0(k), X, FR(k), DA(k), W(k), d, a1, a0));
+    }
+    return MPSB_OK;
+  };
+  // boundaries: the coefficients sit on the right end, or on the left end for mode 2
+  for (int l = 0; l < np; ++l) {
+    MPSB_TRY(set_boundary(ctx, FL2(l, 0), mode == 2 ? coef[l] : ONE_));
+    MPSB_TRY(set_boundary(ctx, FR2(l, na), mode == 2 ? ONE_ : coef[l]));
   }
-  MPSB_TRY(set_boundary(ctx, FR(na), ONE_));
+  if (hasH) {
+    // the 3-index left environment is stored conjugated: conj(coef) there applies coef
+    MPSB_TRY(set_boundary(ctx, FL(0), mode == 2 ? cconj(coef[numv - 1]) : ONE_));
+    MPSB_TRY(set_boundary(ctx, FR(na), mode == 2 ? ONE_ : coef[numv - 1]));
+  }
+  if (mode == 2) {
+    for (int k = na - 1; k >= 2; --k) MPSB_TRY(right_update(k, (int)dims[k], (int)dims[k + 1]));
+  } else {
+    for (int k = 0; k < na - 2; ++k) MPSB_TRY(left_update(k, (int)dims[k], (int)dims[k + 1]));
+  }
   std::vector<double> S;
   // the pair tensor of sites (j, j+1) into av: (dims[j] d) x (d dims[j+2])
   auto pair = [&](int j) -> int {
     const int b0 = (int)dims[j + 2], a0 = (int)dims[j];
+    for (int l = 0; l < np; ++l) {
+      // X[c, s2, b0] = A_l[j+1] FR_l[j+2];  Y[a, s1, (s2 b0)] = A_l[j] X;  av (+)= FL_l[j] Y
+      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(j + 1), FR2(l, j + 2), X, DA(j + 1) * d, DA(j + 2), b0, ONE_, ZERO_));
+      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(j), X, Y, DA(j) * d, DA(j + 1), d * b0, ONE_, ZERO_));
+      MPSB_TRY(op_L2_A3(ctx, FL2(l, j), Y, av, a0, DA(j), d * d * b0, ONE_, l ? ONE_ : ZERO_, false));
+    }
+    if (!hasH) return MPSB_OK;
     // X[c, v, s2, b0] = prod_AOR(A[j+1], H[j+1], FR[j+2])
     MPSB_TRY(op_prod_AOR(ctx, A->site(j + 1), H->site(j + 1), FR(j + 2), X, DA(j + 1), d, DA(j + 2), W(j + 1), W(j + 2), b0));
     // Y[a, w, s1, (s2 b0)] = prod_AOR(A[j], H[j], X as R[c, v, (s2 b0)])
     MPSB_TRY(op_prod_AOR(ctx, A->site(j), H->site(j), X, Y, DA(j), d, DA(j + 1), W(j), W(j + 1), d * b0));
-    // av[a0, s1, (s2 b0)] = sum_{a, w} conj(L[a, w, a0]) Y[a, w, s1, (s2 b0)]
-    return op_prod_LR_3_4(ctx, FL(j), Y, av, DA(j), W(j), a0, d, d * b0, ONE_, cmk(0.0, 0.0));
+    // av[a0, s1, (s2 b0)] (+)= sum_{a, w} conj(L[a, w, a0]) Y[a, w, s1, (s2 b0)]
+    return op_prod_LR_3_4(ctx, FL(j), Y, av, DA(j), W(j), a0, d, d * b0, ONE_, np ? ONE_ : ZERO_);
   };
   auto svd_pair = [&](int j, int& k) -> int {
     const int m = (int)dims[j] * d, n = d * (int)dims[j + 2];
@@ -438,8 +502,8 @@ int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, con
     return svd_launch(m, n, av, 1, m, U, 1, m, S.data(), V, 1, n, &ctx->ws, st);
   };
   int k = 0, dnew = 1;
-  for (int sweep = 0; sweep < maxsweeps; ++sweep) {
-    for (int j = na - 2; j >= 0; --j) {   // sweep left: pairs (j, j+1), site j+1 becomes V'
+  auto sweep_left = [&]() -> int {   // pairs (j, j+1) from the right end, site j+1 becomes V'
+    for (int j = na - 2; j >= 0; --j) {
       MPSB_TRY(pair(j));
       MPSB_TRY(svd_pair(j, k));
       dnew = truncation_rule(S, k, svd_tol, dlim);
@@ -449,12 +513,12 @@ int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, con
       count_launch(&ctx->ws);
       sv_adjoint_kernel<<<148 * 2, 256, 0, st>>>(dnew, n, V, n, nullptr, site0(j + 1));
       MPSB_CUDA_TRY(cudaGetLastError());
-      // FR[j+1] = update_re(A0[j+1], H[j+1], A[j+1], FR[j+2])
-      MPSB_TRY(op_prod_AOR(ctx, A->site(j + 1), H->site(j + 1), FR(j + 2), X, DA(j + 1), d, DA(j + 2), W(j + 1),
-                           W(j + 2), (int)dims[j + 2]));
-      MPSB_TRY(op_update_re(ctx, site0(j + 1), X, FR(j + 1), DA(j + 1), W(j + 1), d, (int)dims[j + 2], dnew));
+      MPSB_TRY(right_update(j + 1, dnew, (int)dims[j + 2]));
     }
-    for (int j = 0; j <= na - 2; ++j) {   // sweep right: site j becomes U
+    return MPSB_OK;
+  };
+  auto sweep_right = [&]() -> int {   // pairs from the left end, site j becomes U
+    for (int j = 0; j <= na - 2; ++j) {
       MPSB_TRY(pair(j));
       MPSB_TRY(svd_pair(j, k));
       dnew = truncation_rule(S, k, svd_tol, dlim);
@@ -462,20 +526,50 @@ int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, con
       dims[j + 1] = dnew;
       const int m = (int)dims[j] * d;
       MPSB_CUDA_TRY(cudaMemcpyAsync(site0(j), U, (size_t)m * dnew * sizeof(cd), cudaMemcpyDeviceToDevice, st));
-      // FL[j+1] = update_le(A0[j], H[j], A[j], FL[j])
-      MPSB_TRY(op_prod_AOL(ctx, A->site(j), H->site(j), FL(j), Y, DA(j), d, DA(j + 1), W(j), W(j + 1), (int)dims[j]));
-      MPSB_TRY(op_update_le(ctx, site0(j), Y, FL(j + 1), (int)dims[j], d, DA(j + 1), W(j + 1), dnew));
+      MPSB_TRY(left_update(j, (int)dims[j], dnew));
     }
-    // last site: diag(S) V' of the last pair
+    return MPSB_OK;
+  };
+  // last site of a L->R sweep: diag(S) V' of the last pair
+  auto close_right = [&]() -> int {
     const int n = d * (int)dims[na];
     MPSB_CUDA_TRY(cudaMemcpyAsync(dS, S.data(), dnew * sizeof(double), cudaMemcpyHostToDevice, st));
     count_launch(&ctx->ws);
     sv_adjoint_kernel<<<148 * 2, 256, 0, st>>>(dnew, n, V, n, dS, site0(na - 1));
     MPSB_CUDA_TRY(cudaGetLastError());
+    return MPSB_OK;
+  };
+  if (mode == 0) {
+    for (int sweep = 0; sweep < maxsweeps; ++sweep) {
+      MPSB_TRY(sweep_left());
+      MPSB_TRY(sweep_right());
+      MPSB_TRY(close_right());
+    }
+  } else if (mode == 1) {
+    MPSB_TRY(sweep_left());
+    // first site: U diag(S) of the last pair
+    const int m = (int)dims[0] * d;
+    MPSB_CUDA_TRY(cudaMemcpyAsync(dS, S.data(), dnew * sizeof(double), cudaMemcpyHostToDevice, st));
+    count_launch(&ctx->ws);
+    scale_cols_kernel<<<148 * 2, 256, 0, st>>>(m, dnew, U, dS, site0(0));
+    MPSB_CUDA_TRY(cudaGetLastError());
+  } else {
+    MPSB_TRY(sweep_right());
+    MPSB_TRY(close_right());
   }
   dims_out = dims;
   *sites = A0;
   return MPSB_OK;
+}
+
+// compress_var_apply_H_two_site (src/compression.jl:355-411): one term through H, coefficient 1
+int compress_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const mpsb_mps* A, const mpsb_mpo* H, int maxsweeps,
+                      double svd_tol, int dlim, std::vector<int64_t>& dims_out, std::vector<int64_t>& offs,
+                      cd** sites) {
+  if (!H) return MPSB_ERR_INVALID_ARG;
+  const cd one = cmk(1.0, 0.0);
+  const mpsb_mps* terms[1] = {A};
+  return compress_two_site_sum(ctx, Ain, 1, &one, terms, H, maxsweeps, svd_tol, dlim, 0, dims_out, offs, sites);
 }
 
 }  // namespace mpsb

@@ -210,6 +210,25 @@ function compress_var_apply_H_two_site(ctx::Ctx, Ain::DMPS, A::DMPS, H::DMPO, ma
     return wrap_new_mps(out[])
 end
 
+# compress_sum_var_apply_H_two_site(Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim)   src/compression.jl:1072-1157
+# half = 1: the _left form (:1159-1215), half = 2: the _right form (:1218-1276); H = nothing:
+# compress_sum_var_two_site (:574-648).  Returns the compressed MPS (new handle, updated dims).
+function compress_sum_var_apply_H_two_site(ctx::Ctx, Ain::DMPS, coef::Vector{<:Number}, A::Vector{DMPS},
+                                           H::Union{DMPO,Nothing}, maxsweeps::Integer, svd_tol::Real,
+                                           dlim::Integer; half::Integer = 0)
+    c = ComplexF64.(coef)
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:mpsb_compress_sum_var_apply_H_two_site, LIB), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{ComplexF64}, Cint, Ptr{Ptr{Cvoid}}, Ptr{Cvoid}, Cint, Cdouble, Cint, Cint,
+                 Ptr{Ptr{Cvoid}}),
+                ctx.h, Ain.h, c, length(c), [a.h for a in A], H === nothing ? C_NULL : H.h, maxsweeps, svd_tol, dlim,
+                half, out), :mpsb_compress_sum_var_apply_H_two_site)
+    return wrap_new_mps(out[])
+end
+compress_sum_var_two_site(ctx::Ctx, Ain::DMPS, coef::Vector{<:Number}, A::Vector{DMPS}, maxsweeps::Integer,
+                          svd_tol::Real, dlim::Integer) =
+    compress_sum_var_apply_H_two_site(ctx, Ain, coef, A, nothing, maxsweeps, svd_tol, dlim)
+
 # Two-lane RK4 step on (1, default) or off (0); no reference counterpart (results are identical)
 set_pipeline!(ctx::Ctx, enable::Bool) =
     check(ccall((:mpsb_ctx_set_pipeline, LIB), Cint, (Ptr{Cvoid}, Cint), ctx.h, enable ? 1 : 0),

@@ -78,6 +78,7 @@ SIGNATURES = {
     "mpsb_op_update_le": ([_vp] * 4 + [_i] * 5, _i),
     "mpsb_compression_svd": ([_vp, _vp, _i, _d, _pvp, _pd, _pd, _pd], _i),
     "mpsb_compress_var_apply_H_two_site": ([_vp, _vp, _vp, _vp, _i, _d, _i, _pvp], _i),
+    "mpsb_compress_sum_var_apply_H_two_site": ([_vp, _vp, _pd, _i, _pvp, _vp, _i, _d, _i, _i, _pvp], _i),
     "mpsb_op_svd": ([_vp, _vp, _vp, _pd, _vp, _i, _i], _i),
     "mpsb_op_qr": ([_vp] * 4 + [_i] * 2, _i),
     "mpsb_op_prod_AOR_noalloc": ([_vp] * 5 + [_i] * 6, _i),

@@ -510,6 +510,39 @@ def compress_var_two_site(Ain, A, maxsweeps, svd_tol, dims, dlim):
     return compress_var_apply_H_two_site(Ain, A, Id, maxsweeps, svd_tol, dims, dlim)
 
 
+def _sum_two_site(name, Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim, half):
+    numv, cb, terms = _terms(name, coef, A)
+    out = C.c_void_p()
+    _lib.call("mpsb_compress_sum_var_apply_H_two_site", Ain.ctx.h, Ain.h, _dptr(cb), numv, terms,
+              H.h if H is not None else None, int(maxsweeps), float(svd_tol), int(dlim), int(half), C.byref(out))
+    new = _wrap_new_mps(out, Ain.ctx, Ain.na, Ain.d)
+    dims[:] = new.dims
+    return new
+
+
+def compress_sum_var_apply_H_two_site(Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:1072-1157: two-site variational compression of
+    sum_l coef[l] A[l] + coef[-1] H A[-1] (guess Ain, left canonical).  Returns the new MPS;
+    `dims` is updated in place."""
+    return _sum_two_site("compress_sum_var_apply_H_two_site", Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim, 0)
+
+
+def compress_sum_var_apply_H_two_site_left(Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:1159-1215: one right-to-left two-site sweep (first site U diag(S))."""
+    return _sum_two_site("compress_sum_var_apply_H_two_site_left", Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim, 1)
+
+
+def compress_sum_var_apply_H_two_site_right(Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:1218-1276: one left-to-right two-site sweep from a right-canonical
+    guess (coefficients on the left boundary; last site diag(S) V')."""
+    return _sum_two_site("compress_sum_var_apply_H_two_site_right", Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim, 2)
+
+
+def compress_sum_var_two_site(Ain, coef, A, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:574-648: the same with every term plain (no operator)."""
+    return _sum_two_site("compress_sum_var_two_site", Ain, coef, A, None, maxsweeps, svd_tol, dims, dlim, 0)
+
+
 # ------------------------------------------------------------------ norms, gauge, observables
 
 def _scalar(name, *args):

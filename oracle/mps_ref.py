@@ -799,5 +799,100 @@ def compress_var_apply_H_two_site(Ain, A, H, maxsweeps, svd_tol, dims, dlim):
     return A0
 
 
+def compress_sum_var_apply_H_two_site(Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim, mode=0):
+    """src/compression.jl:1072-1157 (mode 0), its _left form :1159-1215 (mode 1: one R->L
+    sweep, first site U diag(S)) and _right form :1218-1276 (mode 2: one L->R sweep from right
+    environments of a right-canonical Ain, coefficients on the left boundary); with H None,
+    compress_sum_var_two_site :574-648 (every term plain).  The pair tensor is
+    sum_l FL_l A_l1 A_l2 FR_l + sum conj(L) A1 O1 A2 O2 R with the 2-index left environment
+    contracted on its A index (the single-site convention; the reference's
+    A_prod_LR_two_site, src/MatrixProductStates.jl:288-292, contracts it transposed) and
+    `svdecon` as the thin SVD.  dims is updated in place."""
+    na = len(Ain)
+    numv = len(coef)
+    np_ = numv - 1 if H is not None else numv
+    AH = A[numv - 1]
+    d = AH[0].shape[1]
+    one2 = np.ones((1, 1), dtype=CT)
+    one3 = np.ones((1, 1, 1), dtype=CT)
+    FL2 = [[None] * (na + 1) for _ in range(np_)]
+    FR2 = [[None] * (na + 1) for _ in range(np_)]
+    FL, FR = [None] * (na + 1), [None] * (na + 1)
+    for l in range(np_):
+        FL2[l][0] = coef[l] * one2 if mode == 2 else one2
+        FR2[l][na] = one2 if mode == 2 else coef[l] * one2
+    if H is not None:
+        # the 3-index left environment is stored conjugated: conj(coef) there applies coef
+        FL[0] = np.conj(coef[-1]) * one3 if mode == 2 else one3
+        FR[na] = one3 if mode == 2 else coef[-1] * one3
+    A0 = copy_mps(Ain)
+
+    def left_update(k):                       # FL[k+1] from A0[k]
+        for l in range(np_):
+            FL2[l][k + 1] = update_lenv_full(A0[k], A[l][k], FL2[l][k])
+        if H is not None:
+            FL[k + 1] = update_le_full(A0[k], H[k], AH[k], FL[k])
+
+    def right_update(k):                      # FR[k] from A0[k]
+        for l in range(np_):
+            FR2[l][k] = update_renv_full(A0[k], A[l][k], FR2[l][k + 1])
+        if H is not None:
+            FR[k] = update_re_full(A0[k], H[k], AH[k], FR[k + 1])
+
+    if mode == 2:
+        for k in range(na - 1, 1, -1):
+            right_update(k)
+    else:
+        for k in range(na - 2):
+            left_update(k)
+
+    def pair(j):
+        av = 0
+        for l in range(np_):
+            t = np.einsum("xa,asc,ctb,by->xsty", FL2[l][j], A[l][j], A[l][j + 1], FR2[l][j + 2])
+            av = av + t.reshape(t.shape[0], d, -1, order="F")
+        if H is not None:
+            X = prod_AOR(AH[j + 1], H[j + 1], FR[j + 2])
+            R2 = X.reshape(X.shape[0], X.shape[1], -1, order="F")
+            Y = prod_AOR(AH[j], H[j], R2)
+            av = av + np.einsum("awx,awsy->xsy", FL[j].conj(), Y)
+        return av.reshape(av.shape[0] * d, -1, order="F")
+
+    def sweep_left():
+        out = None
+        for j in range(na - 2, -1, -1):
+            u, s, vh = np.linalg.svd(pair(j), full_matrices=False)
+            dn = _trunc_rule(s, svd_tol, dlim)
+            dims[j + 1] = dn
+            A0[j + 1] = jr(vh[:dn, :], dn, d, dims[j + 2])
+            right_update(j + 1)
+            out = (u, s, dn)
+        return out
+
+    def sweep_right():
+        out = None
+        for j in range(na - 1):
+            u, s, vh = np.linalg.svd(pair(j), full_matrices=False)
+            dn = _trunc_rule(s, svd_tol, dlim)
+            dims[j + 1] = dn
+            A0[j] = jr(u[:, :dn], dims[j], d, dn)
+            left_update(j)
+            out = (s, vh, dn)
+        return out
+
+    if mode == 0:
+        for _ in range(maxsweeps):
+            sweep_left()
+            s, vh, dn = sweep_right()
+            A0[na - 1] = jr(np.diag(s[:dn]) @ vh[:dn, :], dn, d, dims[na])
+    elif mode == 1:
+        u, s, dn = sweep_left()
+        A0[0] = jr(u[:, :dn] @ np.diag(s[:dn]), dims[0], d, dn)
+    else:
+        s, vh, dn = sweep_right()
+        A0[na - 1] = jr(np.diag(s[:dn]) @ vh[:dn, :], dn, d, dims[na])
+    return A0
+
+
 def copy_mps(mps):
     return [np.array(a, dtype=CT, copy=True) for a in mps]

@@ -186,3 +186,37 @@ def test_two_site_compression_matches_oracle(gpu_ctx, dlim, tol, sweeps):
     gd2 = list(dims)
     got2 = K.compress_var_two_site(gA, gA, 1, 1e-14, gd2, dlim)
     assert gd2 == dd2 and 1 - fidelity(got2.sites(), ref2) < 1e-10
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("with_h", [True, False])
+@pytest.mark.parametrize("dlim,tol", [(16, 1e-14), (5, 1e-6)])
+def test_two_site_sum_compression_matches_oracle(gpu_ctx, mode, with_h, dlim, tol):
+    """compress_sum_var_apply_H_two_site with its _left / _right half sweeps, and
+    compress_sum_var_two_site: three complex-weighted terms (the last through H when given),
+    at full bond dimension and truncated; bond dims, norm and fidelity against the oracle."""
+    import mpsb200 as K
+    na = 7
+    rng = np.random.default_rng(60 + mode)
+    terms = [R.mpsrandom(na, 4, 2, rng)[0] for _ in range(3)]
+    coef = [0.7 - 0.2j, -0.4 + 0.9j, 1.3 + 0.1j]
+    H = OM.sm_hamiltonian(OM.SpinChain(na, omega=0.5), 1.0, 0.05, 0.0)
+    guess, dims = R.mpsrandom(na, 8, 2, rng)
+    if mode == 2:
+        R.rightorthogonalizeQR_(guess)
+    dd = list(dims)
+    ref = R.compress_sum_var_apply_H_two_site(R.copy_mps(guess), coef, terms, H if with_h else None, 2, tol, dd,
+                                              dlim, mode)
+    gterms = [K.MPS.from_sites(t, gpu_ctx) for t in terms]
+    gguess = K.MPS.from_sites(guess, gpu_ctx)
+    gd = list(dims)
+    if mode == 0 and not with_h:
+        got = K.compress_sum_var_two_site(gguess, coef, gterms, 2, tol, gd, dlim)
+    else:
+        fn = {0: K.compress_sum_var_apply_H_two_site, 1: K.compress_sum_var_apply_H_two_site_left,
+              2: K.compress_sum_var_apply_H_two_site_right}[mode]
+        gH = K.MPO.from_sites(H, gpu_ctx) if with_h else None   # None: every term plain
+        got = fn(gguess, coef, gterms, gH, 2, tol, gd, dlim)
+    assert gd == dd and got.dims == dd
+    assert 1 - fidelity(got.sites(), ref) < 1e-10
+    assert abs(R.scal_prod(got.sites(), got.sites()) / R.scal_prod(ref, ref) - 1) < 1e-10

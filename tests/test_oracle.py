@@ -369,3 +369,45 @@ def test_two_site_compression_exact_at_full_bond_dimension():
     want = D.mpo_to_dense(H) @ D.mps_to_dense(A)
     assert np.linalg.norm(D.mps_to_dense(out) - want) < 1e-12 * np.linalg.norm(want)
     assert dd == [1, 2, 4, 8, 16, 8, 4, 2, 1]
+
+
+def _two_site_sum_case(na=6, seed=11):
+    rng = np.random.default_rng(seed)
+    terms = [R.mpsrandom(na, 4, 2, rng)[0] for _ in range(3)]
+    coef = [0.7 - 0.2j, -0.4 + 0.9j, 1.3 + 0.1j]
+    H = M.sm_hamiltonian(M.SpinChain(na, omega=0.5), 1.0, 0.05, 0.0)
+    plain = sum(c * D.mps_to_dense(t) for c, t in zip(coef[:-1], terms[:-1]))
+    with_h = plain + coef[-1] * (D.mpo_to_dense(H) @ D.mps_to_dense(terms[-1]))
+    all_plain = plain + coef[-1] * D.mps_to_dense(terms[-1])
+    return rng, terms, coef, H, with_h, all_plain
+
+
+def test_two_site_sum_single_term_is_the_two_site_compression():
+    na = 6
+    rng = np.random.default_rng(4)
+    A, dims = R.mpsrandom(na, 4, 2, rng)
+    H = M.sm_hamiltonian(M.SpinChain(na, omega=0.5), 1.0, 0.05, 0.0)
+    d1, d2 = list(dims), list(dims)
+    a = R.compress_var_apply_H_two_site(R.copy_mps(A), A, H, 2, 1e-10, d1, 6)
+    b = R.compress_sum_var_apply_H_two_site(R.copy_mps(A), [1.0], [A], H, 2, 1e-10, d2, 6)
+    assert d1 == d2
+    assert max(np.abs(x - y).max() for x, y in zip(a, b)) < 1e-14
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("with_h", [True, False])
+def test_two_site_sum_exact_at_full_bond_dimension(mode, with_h):
+    """compress_sum_var_apply_H_two_site (src/compression.jl:1072-1157), its _left / _right
+    half sweeps (:1159-1276) and compress_sum_var_two_site (:574-648): from a guess at the
+    full bond dimension (left canonical; right canonical for the L->R half sweep) and with no
+    truncation, the result is the exact sum of the terms."""
+    na = 6
+    rng, terms, coef, H, want_h, want_p = _two_site_sum_case(na)
+    guess, dims = R.mpsrandom(na, 8, 2, rng)
+    if mode == 2:
+        R.rightorthogonalizeQR_(guess)
+    dd = list(dims)
+    out = R.compress_sum_var_apply_H_two_site(guess, coef, terms, H if with_h else None, 1, 1e-14, dd, 16, mode)
+    want = want_h if with_h else want_p
+    assert np.linalg.norm(D.mps_to_dense(out) - want) < 1e-10 * np.linalg.norm(want)
+    assert dd == [1, 2, 4, 8, 4, 2, 1]
