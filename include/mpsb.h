@@ -244,8 +244,8 @@ int mpsb_compress_var_apply_H_two_site(mpsb_ctx* ctx, const mpsb_mps* Ain, const
  *   conjugated, so the result is the stated sum also for complex coefficients);
  * compress_sum_var_two_site(Ain, coef, A, maxsweeps, svd_tol, dims, dlim)  :574-648 when H is NULL.
  * Two-site variational compression of sum_l coef[l] A[l], the last term through H when H is
- * given; coef is numv interleaved complex (numv plain terms at most 8 besides the H term); every
- * A[l] has the bond dims of A[numv-1]; Ain is the left-canonical guess (right-canonical for
+ * given; coef is numv interleaved complex (at most 8 plain terms besides the H term); the terms
+ * may have different bond dims; Ain is the left-canonical guess (right-canonical for
  * half = 2).  Bond dims adapt (<= dlim): the result is a new handle *out.  As in
  * mpsb_compress_var_apply_H_two_site the undefined `svdecon` is the thin SVD and the pair
  * contractions use the environments as the single-site path does (the reference's

@@ -363,8 +363,8 @@ int truncation_rule(const std::vector<double>& S, int k, double tol, int dlim) {
 // coefficients on the right boundary); mode 1: one R->L half sweep (the _left form, last site
 // U diag(S)); mode 2: one L->R half sweep from right environments of a right-canonical guess
 // (the _right form, coefficients on the left boundary, last site diag(S) V').  Bond dims
-// change; the result lands in context scratch (site k at offs[k]) with dims_out.  Every A[l]
-// has the bond dims of A[numv-1].
+// change; the result lands in context scratch (site k at offs[k]) with dims_out.  The terms
+// may have different bond dims (the stages of a two-site RK4 step do).
 int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd* coef, const mpsb_mps* const* Av,
                           const mpsb_mpo* H, int maxsweeps, double svd_tol, int dlim, int mode,
                           std::vector<int64_t>& dims_out, std::vector<int64_t>& offs, cd** sites) {
@@ -381,7 +381,7 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
   if (Ain->na != na || Ain->d != d || na < 2) return MPSB_ERR_DIMENSION;
   if (hasH && (H->na != na || H->d != d)) return MPSB_ERR_DIMENSION;
   for (int l = 0; l < numv; ++l)
-    if (Av[l]->na != na || Av[l]->d != d || Av[l]->dims != A->dims) return MPSB_ERR_DIMENSION;
+    if (Av[l]->na != na || Av[l]->d != d) return MPSB_ERR_DIMENSION;
   cudaStream_t st = ctx->stream;
   std::vector<int64_t> dims = Ain->dims, cap(na + 1);
   for (int k = 0; k <= na; ++k) {   // capacity of bond k: the dims rule bound with dlim
@@ -391,12 +391,13 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
     cap[k] = std::max<int64_t>(dims[k], std::min(c, std::min(pl, pr)));
   }
   auto DA = [&](int k) { return (int)A->dims[k]; };
+  auto DL = [&](int l, int k) { return (int)Av[l]->dims[k]; };   // bond k of plain term l
   auto W = [&](int k) { return hasH ? (int)H->w[k] : 1; };
   // scratch: A0 sites at capacity, the FL / FR stacks (3-index for the H term, 2-index for each
   // plain term), two contraction buffers, the pair tensor and the SVD factors
   offs.assign(na, 0);
   int64_t tot = 0, envtot = 0, env2tot = 0, pairmax = 1, aor = 1;
-  std::vector<int64_t> eoff(na + 1), e2off(na + 1);
+  std::vector<int64_t> eoff(na + 1), e2off((size_t)np * (na + 1));
   for (int k = 0; k < na; ++k) {
     offs[k] = tot;
     tot += cap[k] * d * cap[k + 1];
@@ -404,8 +405,21 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
   for (int k = 0; k <= na; ++k) {
     eoff[k] = envtot;
     envtot += (int64_t)DA(k) * W(k) * cap[k];
-    e2off[k] = env2tot;
-    env2tot += (int64_t)DA(k) * cap[k];
+  }
+  for (int l = 0; l < np; ++l)   // plain term l: its FL then its FR stack
+    for (int k = 0; k <= na; ++k) {
+      e2off[(size_t)l * (na + 1) + k] = env2tot;
+      env2tot += 2 * (int64_t)DL(l, k) * cap[k];
+    }
+  for (int l = 0; l < np; ++l) {   // the plain terms' contraction temporaries
+    for (int k = 0; k + 1 < na; ++k) {
+      aor = std::max<int64_t>(aor, (int64_t)DL(l, k) * d * d * cap[k + 2]);
+      aor = std::max<int64_t>(aor, (int64_t)DL(l, k + 1) * d * cap[k + 2]);
+    }
+    for (int k = 0; k < na; ++k) {
+      aor = std::max<int64_t>(aor, (int64_t)DL(l, k) * d * cap[k + 1]);
+      aor = std::max<int64_t>(aor, (int64_t)cap[k] * d * DL(l, k + 1));
+    }
   }
   for (int k = 0; k + 1 < na; ++k) {
     pairmax = std::max<int64_t>(pairmax, cap[k] * d * d * cap[k + 2]);
@@ -416,15 +430,14 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
     aor = std::max<int64_t>(aor, (int64_t)DA(k) * W(k) * d * cap[k + 1]);
     aor = std::max<int64_t>(aor, (int64_t)cap[k] * d * DA(k + 1) * W(k + 1));
   }
-  const size_t need = (size_t)tot + 2 * (hasH ? envtot : 0) + 2 * (size_t)np * env2tot + 2 * aor + 3 * pairmax +
-                      pairmax / 2 + 64;
+  const size_t need = (size_t)tot + 2 * (hasH ? envtot : 0) + (size_t)env2tot + 2 * aor + 3 * pairmax + pairmax / 2 + 64;
   cd* base = nullptr;
   MPSB_TRY(ensure_slot(ctx, SLOT_MISC, need * sizeof(cd), &base));
   cd* A0 = base;
   cd* FLb = A0 + tot;
   cd* FRb = FLb + (hasH ? envtot : 0);
-  cd* F2b = FRb + (hasH ? envtot : 0);   // [np][2][env2tot]: FL_l then FR_l
-  cd* X = F2b + 2 * (size_t)np * env2tot;
+  cd* F2b = FRb + (hasH ? envtot : 0);   // the plain terms' stacks (e2off)
+  cd* X = F2b + env2tot;
   cd* Y = X + aor;
   cd* av = Y + aor;
   cd* U = av + pairmax;
@@ -432,8 +445,8 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
   double* dS = reinterpret_cast<double*>(V + pairmax);
   auto FL = [&](int k) { return FLb + eoff[k]; };
   auto FR = [&](int k) { return FRb + eoff[k]; };
-  auto FL2 = [&](int l, int k) { return F2b + (2 * (int64_t)l) * env2tot + e2off[k]; };
-  auto FR2 = [&](int l, int k) { return F2b + (2 * (int64_t)l + 1) * env2tot + e2off[k]; };
+  auto FL2 = [&](int l, int k) { return F2b + e2off[(size_t)l * (na + 1) + k]; };
+  auto FR2 = [&](int l, int k) { return FL2(l, k) + (int64_t)DL(l, k) * cap[k]; };
   auto site0 = [&](int k) { return A0 + offs[k]; };
   const cd ONE_ = cmk(1.0, 0.0), ZERO_ = cmk(0.0, 0.0);
   for (int k = 0; k < na; ++k)   // A0 starts as the guess (dims of Ain)
@@ -442,8 +455,8 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
   // environment updates from site k of A0 (bond dims a0 -> a1 of A0)
   auto left_update = [&](int k, int a0, int a1) -> int {   // FL[k+1] from FL[k]
     for (int l = 0; l < np; ++l) {
-      MPSB_TRY(op_L2_A3(ctx, FL2(l, k), Av[l]->site(k), X, a0, DA(k), d * DA(k + 1), ONE_, ZERO_, false));
-      MPSB_TRY(op_update_lenv(ctx, site0(k), X, FL2(l, k + 1), a0 * d, a1, DA(k + 1), true));
+      MPSB_TRY(op_L2_A3(ctx, FL2(l, k), Av[l]->site(k), X, a0, DL(l, k), d * DL(l, k + 1), ONE_, ZERO_, false));
+      MPSB_TRY(op_update_lenv(ctx, site0(k), X, FL2(l, k + 1), a0 * d, a1, DL(l, k + 1), true));
     }
     if (hasH) {
       MPSB_TRY(op_prod_AOL(ctx, A->site(k), H->site(k), FL(k), Y, DA(k), d, DA(k + 1), W(k), W(k + 1), a0));
@@ -453,8 +466,8 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
   };
   auto right_update = [&](int k, int a0, int a1) -> int {   // FR[k] from FR[k+1]
     for (int l = 0; l < np; ++l) {
-      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(k), FR2(l, k + 1), X, DA(k) * d, DA(k + 1), a1, ONE_, ZERO_));
-      MPSB_TRY(op_update_renv(ctx, site0(k), X, FR2(l, k), DA(k), a0, d * a1));
+      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(k), FR2(l, k + 1), X, DL(l, k) * d, DL(l, k + 1), a1, ONE_, ZERO_));
+      MPSB_TRY(op_update_renv(ctx, site0(k), X, FR2(l, k), DL(l, k), a0, d * a1));
     }
     if (hasH) {
       MPSB_TRY(op_prod_AOR(ctx, A->site(k), H->site(k), FR(k + 1), X, DA(k), d, DA(k + 1), W(k), W(k + 1), a1));
@@ -483,9 +496,9 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
     const int b0 = (int)dims[j + 2], a0 = (int)dims[j];
     for (int l = 0; l < np; ++l) {
       // X[c, s2, b0] = A_l[j+1] FR_l[j+2];  Y[a, s1, (s2 b0)] = A_l[j] X;  av (+)= FL_l[j] Y
-      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(j + 1), FR2(l, j + 2), X, DA(j + 1) * d, DA(j + 2), b0, ONE_, ZERO_));
-      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(j), X, Y, DA(j) * d, DA(j + 1), d * b0, ONE_, ZERO_));
-      MPSB_TRY(op_L2_A3(ctx, FL2(l, j), Y, av, a0, DA(j), d * d * b0, ONE_, l ? ONE_ : ZERO_, false));
+      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(j + 1), FR2(l, j + 2), X, DL(l, j + 1) * d, DL(l, j + 2), b0, ONE_, ZERO_));
+      MPSB_TRY(op_A3_R2(ctx, Av[l]->site(j), X, Y, DL(l, j) * d, DL(l, j + 1), d * b0, ONE_, ZERO_));
+      MPSB_TRY(op_L2_A3(ctx, FL2(l, j), Y, av, a0, DL(l, j), d * d * b0, ONE_, l ? ONE_ : ZERO_, false));
     }
     if (!hasH) return MPSB_OK;
     // X[c, v, s2, b0] = prod_AOR(A[j+1], H[j+1], FR[j+2])

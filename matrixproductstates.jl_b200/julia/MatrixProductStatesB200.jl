@@ -229,6 +229,18 @@ compress_sum_var_two_site(ctx::Ctx, Ain::DMPS, coef::Vector{<:Number}, A::Vector
                           svd_tol::Real, dlim::Integer) =
     compress_sum_var_apply_H_two_site(ctx, Ain, coef, A, nothing, maxsweeps, svd_tol, dlim)
 
+# RK4stp_apply_H_half_full_two_site(dt, H, psi, svd_tol, dims, dlim)   src/timeevolution.jl:208-215
+# Four two-site half sweeps with adapting bonds; returns the new psi (its `dims` field holds
+# the reference's updated dims).
+function RK4stp_apply_H_half_full_two_site(ctx::Ctx, dt::Real, H::Vector{DMPO}, psi::DMPS, svd_tol::Real,
+                                           dlim::Integer)
+    s(Ain, c, A, O, half) = compress_sum_var_apply_H_two_site(ctx, Ain, c, A, O, 1, svd_tol, dlim; half = half)
+    psi1 = s(psi, [1.0], [psi], H[1], 1)
+    psi2 = s(psi1, [1.0, dt / 2], [psi, psi1], H[2], 2)
+    psi3 = s(psi2, [1.0, dt], [psi, psi2], H[2], 1)
+    return s(psi3, [-1 / 3, 1 / 3, 2 / 3, 1 / 3], [psi, psi1, psi2, psi3], H[3], 2)
+end
+
 # Two-lane RK4 step on (1, default) or off (0); no reference counterpart (results are identical)
 set_pipeline!(ctx::Ctx, enable::Bool) =
     check(ccall((:mpsb_ctx_set_pipeline, LIB), Cint, (Ptr{Cvoid}, Cint), ctx.h, enable ? 1 : 0),

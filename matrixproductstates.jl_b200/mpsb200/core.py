@@ -538,6 +538,28 @@ def compress_sum_var_apply_H_two_site_right(Ain, coef, A, H, maxsweeps, svd_tol,
     return _sum_two_site("compress_sum_var_apply_H_two_site_right", Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim, 2)
 
 
+def compress_var_apply_H_two_site_left(Ain, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:413-448: one right-to-left two-site sweep of H*A (first site U diag(S))."""
+    return compress_sum_var_apply_H_two_site_left(Ain, [1.0], [A], H, maxsweeps, svd_tol, dims, dlim)
+
+
+def compress_var_apply_H_two_site_right(Ain, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:450-486: one left-to-right two-site sweep of H*A from a right-canonical
+    guess (last site diag(S) V')."""
+    return compress_sum_var_apply_H_two_site_right(Ain, [1.0], [A], H, maxsweeps, svd_tol, dims, dlim)
+
+
+def RK4stp_apply_H_half_full_two_site(dt, H, psi, svd_tol, dims, dlim):
+    """src/timeevolution.jl:208-215: the RK4 step with every stage a two-site half sweep
+    (R->L, L->R, R->L, L->R), so the bond dims adapt to the state (<= dlim, truncation rule of
+    compressionSVD! with svd_tol); `dims` is updated in place and the new psi returned."""
+    psi1 = compress_var_apply_H_two_site_left(psi, psi, H[0], 1, svd_tol, dims, dlim)
+    psi2 = compress_sum_var_apply_H_two_site_right(psi1, [1.0, dt / 2], [psi, psi1], H[1], 1, svd_tol, dims, dlim)
+    psi3 = compress_sum_var_apply_H_two_site_left(psi2, [1.0, dt], [psi, psi2], H[1], 1, svd_tol, dims, dlim)
+    return compress_sum_var_apply_H_two_site_right(psi3, [-1 / 3, 1 / 3, 2 / 3, 1 / 3], [psi, psi1, psi2, psi3], H[2],
+                                                   1, svd_tol, dims, dlim)
+
+
 def compress_sum_var_two_site(Ain, coef, A, maxsweeps, svd_tol, dims, dlim):
     """src/compression.jl:574-648: the same with every term plain (no operator)."""
     return _sum_two_site("compress_sum_var_two_site", Ain, coef, A, None, maxsweeps, svd_tol, dims, dlim, 0)

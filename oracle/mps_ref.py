@@ -894,5 +894,25 @@ def compress_sum_var_apply_H_two_site(Ain, coef, A, H, maxsweeps, svd_tol, dims,
     return A0
 
 
+def compress_var_apply_H_two_site_left(Ain, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:413-448: the single-term one R->L two-site sweep."""
+    return compress_sum_var_apply_H_two_site(Ain, [1.0], [A], H, maxsweeps, svd_tol, dims, dlim, 1)
+
+
+def compress_var_apply_H_two_site_right(Ain, A, H, maxsweeps, svd_tol, dims, dlim):
+    """src/compression.jl:450-486: the single-term one L->R two-site sweep."""
+    return compress_sum_var_apply_H_two_site(Ain, [1.0], [A], H, maxsweeps, svd_tol, dims, dlim, 2)
+
+
+def RK4stp_apply_H_half_full_two_site(dt, H, psi, svd_tol, dims, dlim):
+    """src/timeevolution.jl:208-215: the RK4 step with every stage a two-site half sweep, the
+    bond dims adapting (dims updated in place); returns the new psi."""
+    psi1 = compress_var_apply_H_two_site_left(psi, psi, H[0], 1, svd_tol, dims, dlim)
+    psi2 = compress_sum_var_apply_H_two_site(psi1, [1, dt / 2], [psi, psi1], H[1], 1, svd_tol, dims, dlim, 2)
+    psi3 = compress_sum_var_apply_H_two_site(psi2, [1, dt], [psi, psi2], H[1], 1, svd_tol, dims, dlim, 1)
+    return compress_sum_var_apply_H_two_site(psi3, [-1 / 3, 1 / 3, 2 / 3, 1 / 3], [psi, psi1, psi2, psi3], H[2], 1,
+                                             svd_tol, dims, dlim, 2)
+
+
 def copy_mps(mps):
     return [np.array(a, dtype=CT, copy=True) for a in mps]

@@ -220,3 +220,45 @@ def test_two_site_sum_compression_matches_oracle(gpu_ctx, mode, with_h, dlim, to
     assert gd == dd and got.dims == dd
     assert 1 - fidelity(got.sites(), ref) < 1e-10
     assert abs(R.scal_prod(got.sites(), got.sites()) / R.scal_prod(ref, ref) - 1) < 1e-10
+
+
+def test_two_site_sum_terms_of_different_bond_dims(gpu_ctx):
+    """The stages of a two-site RK4 step sum MPSs whose bonds differ: each plain term keeps
+    its own environments."""
+    import mpsb200 as K
+    na = 7
+    rng = np.random.default_rng(71)
+    terms = [R.mpsrandom(na, dm, 2, rng)[0] for dm in (2, 8, 4)]
+    coef = [0.3 + 0.4j, -1.1, 0.5j]
+    H = OM.sm_hamiltonian(OM.SpinChain(na, omega=0.5), 1.0, 0.05, 0.0)
+    guess, dims = R.mpsrandom(na, 4, 2, rng)
+    for mode in (0, 1):
+        dd = list(dims)
+        ref = R.compress_sum_var_apply_H_two_site(R.copy_mps(guess), coef, terms, H, 1, 1e-10, dd, 12, mode)
+        gd = list(dims)
+        fn = K.compress_sum_var_apply_H_two_site if mode == 0 else K.compress_sum_var_apply_H_two_site_left
+        got = fn(K.MPS.from_sites(guess, gpu_ctx), coef, [K.MPS.from_sites(t, gpu_ctx) for t in terms],
+                 K.MPO.from_sites(H, gpu_ctx), 1, 1e-10, gd, 12)
+        assert gd == dd
+        assert 1 - fidelity(got.sites(), ref) < 1e-10
+
+
+@pytest.mark.parametrize("dlim,tol", [(16, 1e-14), (6, 1e-10)])
+def test_two_site_rk4_step_matches_oracle(gpu_ctx, dlim, tol):
+    """RK4stp_apply_H_half_full_two_site: three steps with adapting bonds (and at the full bond
+    dimension, where the oracle equals the dense RK4 map)."""
+    import mpsb200 as K
+    na, dt = 8, 0.01
+    rng = np.random.default_rng(81)
+    psi, dims = R.mpsrandom(na, 4, 2, rng)
+    p = OM.SpinChain(na, omega=0.5)
+    H = [OM.sm_hamiltonian(p, 1, dt / 2, 0), OM.sm_hamiltonian(p, 0, 1, dt / 2), OM.sm_hamiltonian(p, 1, dt / 2, dt)]
+    gH = [K.MPO.from_sites(h, gpu_ctx) for h in H]
+    g = K.MPS.from_sites(psi, gpu_ctx)
+    dd, gd = list(dims), list(dims)
+    for _ in range(3):
+        psi = R.RK4stp_apply_H_half_full_two_site(dt, H, psi, tol, dd, dlim)
+        g = K.RK4stp_apply_H_half_full_two_site(dt, gH, g, tol, gd, dlim)
+        assert gd == dd and g.dims == dd
+        assert 1 - fidelity(g.sites(), psi) < 1e-10
+        assert abs(R.scal_prod(g.sites(), g.sites()) / R.scal_prod(psi, psi) - 1) < 1e-10

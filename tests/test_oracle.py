@@ -411,3 +411,22 @@ def test_two_site_sum_exact_at_full_bond_dimension(mode, with_h):
     want = want_h if with_h else want_p
     assert np.linalg.norm(D.mps_to_dense(out) - want) < 1e-10 * np.linalg.norm(want)
     assert dd == [1, 2, 4, 8, 4, 2, 1]
+
+
+def test_two_site_rk4_step_is_the_dense_rk4_map_at_full_bond_dimension():
+    """RK4stp_apply_H_half_full_two_site (src/timeevolution.jl:208-215): from a left-canonical
+    state at the full bond dimension and without truncation, three steps equal the dense RK4
+    map, and the bonds stay at the full dims."""
+    na, dt = 6, 0.01
+    rng = np.random.default_rng(21)
+    psi, dims = R.mpsrandom(na, 8, 2, rng)
+    p = M.SpinChain(na, omega=0.5)
+    H = [M.sm_hamiltonian(p, 1, dt / 2, 0), M.sm_hamiltonian(p, 0, 1, dt / 2), M.sm_hamiltonian(p, 1, dt / 2, dt)]
+    Hd = [D.mpo_to_dense(h) for h in H]
+    want = D.mps_to_dense(psi)
+    dd = list(dims)
+    for _ in range(3):
+        psi = R.RK4stp_apply_H_half_full_two_site(dt, H, psi, 1e-14, dd, 16)
+        want = D.rk4_dense_step(*Hd, want, dt)
+        assert np.linalg.norm(D.mps_to_dense(psi) - want) < 1e-11 * np.linalg.norm(want)
+    assert dd == [1, 2, 4, 8, 4, 2, 1]
