@@ -9,7 +9,8 @@ from .core import (  # noqa: F401
     build_env, compressionSVD_, compress_sum_var, compress_var_apply_H_two_site, compress_var_two_site,
     compress_sum_var_apply_H_two_site, compress_sum_var_apply_H_two_site_left, compress_sum_var_apply_H_two_site_right,
     compress_sum_var_two_site, compress_var_apply_H_two_site_left, compress_var_apply_H_two_site_right,
-    RK4stp_apply_H_half_full_two_site, compress_sum_var_apply_H_, compress_sum_var_apply_H_left_,
+    RK4stp_apply_H_half_full_two_site, compress_var, compress_var_apply_H, compress_var_apply_H_left,
+    compress_var_apply_H_right, compress_sum_var_apply_H, compress_sum_var_apply_H_left, compress_sum_var_apply_H_right, compress_sum_var_apply_H_, compress_sum_var_apply_H_left_,
     compress_sum_var_apply_H_right_, compress_var_apply_H_,
     compress_var_apply_H_left_, default_context, expandmps, ground_state_search_, leftorth_sites_,
     leftorthogonalizeQR_, product_mpo, steady_state_search_,

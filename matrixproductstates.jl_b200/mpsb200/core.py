@@ -510,6 +510,64 @@ def compress_var_two_site(Ain, A, maxsweeps, svd_tol, dims, dlim):
     return compress_var_apply_H_two_site(Ain, A, Id, maxsweeps, svd_tol, dims, dlim)
 
 
+# The reference's allocating forms: a new output MPS (the guess's dims) and internal
+# environments around the in-place entry points above.
+
+def compress_var(Ain, A, maxsweeps):
+    """src/compression.jl:19-62: a new MPS, the variational compression of A (guess Ain)."""
+    return compress_sum_var(Ain, [1.0], [A], maxsweeps)
+
+
+def _new_like(Ain, H=None, plain=0):
+    A0 = Ain.clone()
+    envop = build_env(Ain.dims, Ain.dims, H.w, Ain.ctx) if H is not None else None
+    env = [build_env(Ain.dims, Ain.dims, None, Ain.ctx) for _ in range(plain)]
+    return A0, envop, env
+
+
+def compress_var_apply_H(Ain, A, H, maxsweeps):
+    """src/compression.jl:173-215: a new MPS compressing H*A with maxsweeps sweep pairs."""
+    A0, envop, _ = _new_like(Ain, H)
+    compress_var_apply_H_(A0, envop, Ain, A, H, maxsweeps)
+    return A0
+
+
+def compress_var_apply_H_left(Ain, A, H):
+    """src/compression.jl:291-319: one right-to-left sweep of H*A from left environments of Ain."""
+    A0, envop, _ = _new_like(Ain, H)
+    compress_var_apply_H_left_(A0, envop, Ain, A, H)
+    return A0
+
+
+def compress_var_apply_H_right(Ain, A, H, maxsweeps=1):
+    """src/compression.jl:261-289: one left-to-right sweep of H*A from right environments of Ain
+    (maxsweeps is unused, as in the reference)."""
+    A0, envop, _ = _new_like(Ain, H)
+    compress_sum_var_apply_H_right_(A0, [], envop, Ain, [1.0], [A], H)
+    return A0
+
+
+def compress_sum_var_apply_H(Ain, coef, A, H, maxsweeps):
+    """src/compression.jl:657-740: a new MPS compressing sum_l coef[l] A[l] + coef[-1] H A[-1]."""
+    A0, envop, _ = _new_like(Ain, H)
+    compress_sum_var_apply_H_(A0, envop, coef, A, H, maxsweeps)
+    return A0
+
+
+def compress_sum_var_apply_H_left(Ain, coef, A, H):
+    """src/compression.jl:742-802: one right-to-left sweep (coefficients on the right boundary)."""
+    A0, envop, env = _new_like(Ain, H, len(coef) - 1)
+    compress_sum_var_apply_H_left_(A0, env, envop, Ain, coef, A, H)
+    return A0
+
+
+def compress_sum_var_apply_H_right(Ain, coef, A, H):
+    """src/compression.jl:946-1005: one left-to-right sweep (coefficients on the left boundary)."""
+    A0, envop, env = _new_like(Ain, H, len(coef) - 1)
+    compress_sum_var_apply_H_right_(A0, env, envop, Ain, coef, A, H)
+    return A0
+
+
 def _sum_two_site(name, Ain, coef, A, H, maxsweeps, svd_tol, dims, dlim, half):
     numv, cb, terms = _terms(name, coef, A)
     out = C.c_void_p()

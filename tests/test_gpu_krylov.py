@@ -262,3 +262,45 @@ def test_two_site_rk4_step_matches_oracle(gpu_ctx, dlim, tol):
         assert gd == dd and g.dims == dd
         assert 1 - fidelity(g.sites(), psi) < 1e-10
         assert abs(R.scal_prod(g.sites(), g.sites()) / R.scal_prod(psi, psi) - 1) < 1e-10
+
+
+def test_allocating_forms_match_oracle(gpu_ctx):
+    """The reference's allocating compressions (compress_var, compress_var_apply_H and its
+    _left / _right, compress_sum_var_apply_H and its _left / _right) return a new MPS equal to
+    the in-place forms run on fresh buffers."""
+    import mpsb200 as K
+    na = 6
+    rng = np.random.default_rng(91)
+    Ain, dims = R.mpsrandom(na, 4, 2, rng)
+    terms = [R.mpsrandom(na, 4, 2, rng)[0] for _ in range(3)]
+    coef = [0.8, -0.3 + 0.2j, 0.6 - 0.1j]
+    H = OM.sm_hamiltonian(OM.SpinChain(na, omega=0.5), 1.0, 0.05, 0.0)
+    w = [h.shape[0] for h in H] + [1]
+    g = lambda x: K.MPS.from_sites(x, gpu_ctx)     # noqa: E731
+    gAin, gterms, gH = g(Ain), [g(t) for t in terms], K.MPO.from_sites(H, gpu_ctx)
+
+    def oracle(fn, *args, plain=0):
+        A0 = R.copy_mps(Ain)
+        envop = R.build_env(dims, dims, w)
+        env = [R.build_env(dims, dims) for _ in range(plain)]
+        fn(A0, *([env] if plain or fn in (R.compress_sum_var_apply_H_right_, R.compress_sum_var_apply_H_left_) else []),
+           envop, *args)
+        return A0
+
+    cases = [
+        (K.compress_var(gAin, gterms[0], 2), R.compress_sum_var(R.copy_mps(Ain), [1.0], [terms[0]], 2)),
+        (K.compress_var_apply_H(gAin, gterms[0], gH, 2), oracle(R.compress_var_apply_H_, Ain, terms[0], H, 2)),
+        (K.compress_var_apply_H_left(gAin, gterms[0], gH), oracle(R.compress_var_apply_H_left_, Ain, terms[0], H)),
+        (K.compress_var_apply_H_right(gAin, gterms[0], gH),   # the oracle's form wants a plain term: weight 0
+         oracle(R.compress_sum_var_apply_H_right_, Ain, [0.0, 1.0], [terms[0], terms[0]], H, plain=1)),
+        (K.compress_sum_var_apply_H(gAin, coef, gterms, gH, 2),
+         oracle(R.compress_sum_var_apply_H_, coef, terms, H, 2)),
+        (K.compress_sum_var_apply_H_left(gAin, coef, gterms, gH),
+         oracle(R.compress_sum_var_apply_H_left_, Ain, coef, terms, H, plain=2)),
+        (K.compress_sum_var_apply_H_right(gAin, coef, gterms, gH),
+         oracle(R.compress_sum_var_apply_H_right_, Ain, coef, terms, H, plain=2)),
+    ]
+    for got, ref in cases:
+        assert got.dims == dims
+        assert 1 - fidelity(got.sites(), ref) < 1e-10
+        assert abs(R.scal_prod(got.sites(), got.sites()) / R.scal_prod(ref, ref) - 1) < 1e-10
