@@ -216,15 +216,6 @@ __device__ __noinline__ Reflector reflector_scaled(const cd* rb, int RS, int C, 
 __device__ __forceinline__ cd shfl(cd v, int src) {
   return cmk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
-__device__ __forceinline__ cd warp_sum(cd v) {
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
-    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
-  }
-  return v;
-}
-
 // ---- per-CTA shared memory map (complex elements) -------------------------------------
 // S     [(ROWS+1) * n]       this CTA's rows, column-major, ld = ROWS+1
 // rcol  [2][C][2*NB]         column exchange (two parities): pq from each rank, row j from its owner
