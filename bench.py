@@ -180,6 +180,22 @@ def oracle_step_rate(nsteps):
     return times
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest of the ranks' x, on every rank (x itself without a process group): the
+    job's time is its slowest replica's."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, sites, steps, secs):
+    """Whole-job site-updates/s: every rank evolves its own replica of `sites` sites."""
+    return world * sites * steps / secs
+
+
 def run_reference(args, rank):
     if rank != 0:
         return None
@@ -345,12 +361,8 @@ def run_ours(args, rank, world, local_rank, dist):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launches = ctx.launches - l0
-    secs = e0.elapsed_time(e1) / 1e3
-    if dist:
-        t = torch.tensor([secs], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        secs = float(t.item())
-    value = world * W["na"] * args.steps / secs
+    secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
+    value = job_rate(world, W["na"], args.steps, secs)
     tr, see, _ = b.observables(pairs=())
 
     # ---- end to end through the public API with host buffers: every step uploads the three
@@ -388,12 +400,8 @@ def run_ours(args, rank, world, local_rank, dist):
     for _ in range(ke):
         e2e_step()
     ctx.sync()
-    e2e_secs = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_secs = float(t.item())
-    e2e_value = world * W["na"] * ke / e2e_secs
+    e2e_secs = max_over_ranks(time.perf_counter() - t0, dist)
+    e2e_value = job_rate(world, W["na"], ke, e2e_secs)
 
     # ---- roofline of the dominant kernel (the cluster QR, ~43% of the step by the ncu launch
     # list) at the workload's interior-site shape, and of the zgemm kernel on the site's GEMMs
