@@ -10,6 +10,11 @@ on the mix: every job's arithmetic is its own (tests/test_gpu_serve.py checks bi
 equality alone vs in the mix).  Reported: per-job latency (arrival to completion) with
 p50/p99, queueing delay, and aggregate site-updates/s.
 
+Failures stay with their job.  A malformed job, or one whose footprint exceeds the whole
+memory budget, is refused at admission (it would otherwise wait forever); a job whose step
+fails (a library error, e.g. a NaN norm) is recorded as failed, its buffers and context are
+released, and the other jobs go on.  Both lists come back in the stats.
+
 The jobs are the reference examples' loops (examples/spin_model_quantum_trajectory_rk4.jl,
 examples/spin_model_density_matrix.jl) as in `drivers`; the uniforms r1/r2 of a trajectory are
 drawn from its own seed.
@@ -19,6 +24,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import _lib
 from . import core as K
 from . import drivers as DR
 from . import models as Mo
@@ -91,6 +97,21 @@ class _Active:
         return {"state": self.buf.A.sites(), "jumps": self.rec["jumps"], "p_coh": np.array(self.rec["p_coh"])}
 
 
+def check_job(job):
+    """Why a job cannot run (None when it can)."""
+    if job.kind not in ("trajectory", "density"):
+        return "unknown kind %r" % (job.kind,)
+    if not (isinstance(job.na, int) and job.na >= 2):
+        return "na must be an integer >= 2"
+    if not (isinstance(job.chi, int) and job.chi >= 1):
+        return "chi must be an integer >= 1"
+    if not (isinstance(job.steps, int) and job.steps >= 1):
+        return "steps must be an integer >= 1"
+    if not (job.dt > 0 and np.isfinite(job.dt)):
+        return "dt must be positive and finite"
+    return None
+
+
 def _start(job, ctx):
     if job.kind == "density":
         p = Mo.WaveguideChain(job.na, gam_eg=0.1, omega=0.5, gam_phi=0.1)
@@ -113,14 +134,32 @@ class Server:
             hbm_bytes = int(0.8 * free)
         self.budget = hbm_bytes
 
-    def run(self, jobs, keep_results=False):
+    def run(self, jobs, keep_results=False, on_admit=None):
+        """Run the stream; `on_admit(active_job)`, when given, is called once per admitted job
+        after its buffers exist (host-side instrumentation and fault injection)."""
         pending = sorted(jobs, key=lambda j: j.arrival)
-        active, done, used = [], [], 0
+        active, done, refused, failed, used = [], [], [], [], 0
         t0 = time.perf_counter()
+
+        def release(a):
+            nonlocal used
+            active.remove(a)
+            used -= footprint(a.job)
+            a.buf = None          # the job's device buffers go before its context
+            a.ctx.close()
+
         while pending or active:
             now = time.perf_counter() - t0
-            while pending and pending[0].arrival <= now and len(active) < self.max_jobs \
-                    and used + footprint(pending[0]) <= self.budget:
+            while pending and pending[0].arrival <= now and len(active) < self.max_jobs:
+                reason = check_job(pending[0])
+                if reason is None and footprint(pending[0]) > self.budget:
+                    reason = "footprint %d bytes exceeds the budget %d" % (footprint(pending[0]), self.budget)
+                if reason is not None:
+                    job = pending.pop(0)
+                    refused.append({"job_id": job.job_id, "reason": reason})
+                    continue
+                if used + footprint(pending[0]) > self.budget:
+                    break
                 job = pending.pop(0)
                 ctx = K.Context(self.device)
                 buf, r1, r2 = _start(job, ctx)
@@ -128,13 +167,26 @@ class Server:
                             rec={"p_coh": [], "jumps": []})
                 active.append(a)
                 used += footprint(job)
+                if on_admit is not None:
+                    on_admit(a)
             if not active:
                 if pending:
                     time.sleep(max(0.0, min(0.01, pending[0].arrival - now)))
                 continue
-            for a in active:
-                a.issue()
-            finished = [a for a in active if a.finish()]
+            for a in list(active):
+                try:
+                    a.issue()
+                except _lib.MpsbError as e:
+                    failed.append({"job_id": a.job.job_id, "step": a.i, "error": str(e)})
+                    release(a)
+            finished = []
+            for a in list(active):
+                try:
+                    if a.finish():
+                        finished.append(a)
+                except _lib.MpsbError as e:
+                    failed.append({"job_id": a.job.job_id, "step": a.i, "error": str(e)})
+                    release(a)
             for a in finished:
                 out = a.result() if keep_results else {}
                 t = time.perf_counter() - t0
@@ -142,17 +194,15 @@ class Server:
                              "steps": a.job.steps, "arrival": a.job.arrival, "admitted": a.admitted,
                              "finished": t, "latency": t - a.job.arrival, "site_updates": a.job.na * a.job.steps,
                              **out})
-                active.remove(a)
-                used -= footprint(a.job)
-                a.buf = None          # the job's device buffers go before its context
-                a.ctx.close()
+                release(a)
         wall = time.perf_counter() - t0
         lat = np.array([r["latency"] for r in done])
         stats = {"jobs": len(done), "wall_s": wall,
-                 "site_updates_per_s": sum(r["site_updates"] for r in done) / wall,
+                 "site_updates_per_s": sum(r["site_updates"] for r in done) / max(wall, 1e-9),
                  "latency_p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
                  "latency_p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
-                 "queue_p50_s": float(np.percentile([r["admitted"] - r["arrival"] for r in done], 50)) if done else None}
+                 "queue_p50_s": float(np.percentile([r["admitted"] - r["arrival"] for r in done], 50)) if done else None,
+                 "refused": refused, "failed": failed}
         return done, stats
 
 

@@ -17,6 +17,45 @@ def test_stream_is_seeded_and_mixed():
     assert all(S.footprint(j) > 0 for j in a)
 
 
+def test_malformed_and_oversize_jobs_are_refused_at_admission():
+    """Host-side failure handling (no device needed: refused jobs never get a context): a
+    malformed descriptor and a job larger than the whole budget are refused with a reason,
+    instead of blocking the stream forever."""
+    from mpsb200 import serve as S
+    jobs = [S.Job("trajectory", 20, 32, 10, job_id=0), S.Job("rk5", 20, 32, 10, job_id=1),
+            S.Job("density", 1, 16, 10, job_id=2), S.Job("trajectory", 20, 32, 0, job_id=3),
+            S.Job("density", 8, 16, 10, dt=float("nan"), job_id=4)]
+    budget = S.footprint(jobs[0]) - 1            # smaller than the one well-formed job
+    done, stats = S.Server(max_jobs=2, hbm_bytes=budget).run(jobs)
+    assert done == [] and stats["failed"] == []
+    reasons = {r["job_id"]: r["reason"] for r in stats["refused"]}
+    assert sorted(reasons) == [0, 1, 2, 3, 4]
+    assert "exceeds the budget" in reasons[0] and "kind" in reasons[1] and "na" in reasons[2]
+    assert "steps" in reasons[3] and "dt" in reasons[4]
+
+
+@pytest.mark.gpu
+def test_a_failing_job_leaves_the_others_intact(gpu_ctx):
+    """Fault injected from the host: one trajectory's Hamiltonian gets a NaN after admission.
+    Its norm check fails (MPSB_ERR_NONFINITE), it is recorded as failed and released, and the
+    other jobs finish with the results they have without it."""
+    from mpsb200 import serve as S
+    jobs = S.poisson_jobs(5, 200.0, 5, kinds=(1.0, 0.0), traj_na=(10, 12), traj_chi=(8, 16), steps=(6, 10))
+    bad = jobs[2].job_id
+
+    def corrupt(a):
+        if a.job.job_id == bad:
+            a.buf.H[0].set_site(0, a.buf.H[0].site(0) * np.nan)
+
+    mixed, stats = S.Server(max_jobs=3).run(jobs, keep_results=True, on_admit=corrupt)
+    assert [f["job_id"] for f in stats["failed"]] == [bad] and "NONFINITE" in stats["failed"][0]["error"]
+    clean, _ = S.Server(max_jobs=3).run([j for j in jobs if j.job_id != bad], keep_results=True)
+    assert sorted(r["job_id"] for r in mixed) == sorted(r["job_id"] for r in clean)
+    for r in mixed:
+        c = next(x for x in clean if x["job_id"] == r["job_id"])
+        assert all(np.array_equal(x, y) for x, y in zip(r["state"], c["state"]))
+
+
 @pytest.mark.gpu
 def test_results_are_the_same_alone_and_in_the_mix(gpu_ctx):
     from mpsb200 import serve as S
