@@ -1,6 +1,7 @@
 """The reference examples' time loops on the GPU engine.
 
-* ``run_trajectory``  examples/spin_model_quantum_trajectory_rk4.jl:44-217
+* ``run_trajectory``  examples/spin_model_quantum_trajectory_rk4.jl:44-217; with order=1
+  examples/spin_model_quantum_trajectory.jl:42-190 (first-order coherent step)
 * ``run_density``     examples/spin_model_density_matrix.jl:36-203 (10-argument in-place RK4)
 
 Every tensor operation is a libmpsb200 call; the host only makes the jump decisions from the
@@ -18,8 +19,8 @@ from . import models as Mo
 class TrajectoryBuffers:
     """Device-resident state of one trajectory (the example's A, A_coh, A_r, A_l, A1..A3, envs)."""
 
-    def __init__(self, p, dmax, dt, ctx=None):
-        self.p, self.dt = p, dt
+    def __init__(self, p, dmax, dt, ctx=None, order=4):
+        self.p, self.dt, self.order = p, dt, order
         na = p.na
         self.A, self.dims = K.mpsgroundstate(na, dmax, 2, ctx)
         ctx = self.A.ctx
@@ -32,13 +33,17 @@ class TrajectoryBuffers:
         self.H = [K.MPO.from_sites(Mo.sm_hamiltonian(p, 1, dt / 2, 0.0), ctx),
                   K.MPO.from_sites(Mo.sm_hamiltonian(p, 0, 1, dt / 2), ctx),
                   K.MPO.from_sites(Mo.sm_hamiltonian(p, 1, dt / 2, dt), ctx)]
+        self.expH = K.MPO.from_sites(Mo.sm_hamiltonian(p, 1, dt, 0.0), ctx) if order == 1 else None
         jr_, jl_ = Mo.jump_mpos(p, 0.0)
         self.jumpright = K.MPO.from_sites(jr_, ctx)
         self.jumpleft = K.MPO.from_sites(jl_, ctx)
 
     def coherent_step(self):
-        K.RK4stp_apply_H_half_(self.dt, self.H, self.A_coh, self.A, self.A1, self.A2, self.A3,
-                               self.env1, self.env2, self.env3, self.envop)
+        if self.order == 1:   # compress_var_apply_H!(A_coh, envop, A, A, expH, 1)
+            K.compress_var_apply_H_(self.A_coh, self.envop, self.A, self.A, self.expH, 1)
+        else:
+            K.RK4stp_apply_H_half_(self.dt, self.H, self.A_coh, self.A, self.A1, self.A2, self.A3,
+                                   self.env1, self.env2, self.env3, self.envop)
         return K.normalize_lo_(self.A_coh)
 
 
@@ -77,8 +82,8 @@ def trajectory_decision(b, i, p_coh, r1, r2, rec):
         rec["jumps"].append((i, "left", 0, p_coh, p_sum))
 
 
-def run_trajectory(p, dmax, dt, nsteps, r1, r2, measure_int=10, ctx=None):
-    b = TrajectoryBuffers(p, dmax, dt, ctx)
+def run_trajectory(p, dmax, dt, nsteps, r1, r2, measure_int=10, ctx=None, order=4):
+    b = TrajectoryBuffers(p, dmax, dt, ctx, order)
     rec = {"p_coh": np.zeros(nsteps), "jumps": [], "e_pop": [K.measure_local(b.A, Mo.E_E)]}
     for i in range(nsteps):
         p_coh = b.coherent_step()

@@ -1,7 +1,9 @@
 """Time loops of the reference examples, restated on the oracle (TEST INFRASTRUCTURE ONLY).
 
 * ``run_trajectory``  examples/spin_model_quantum_trajectory_rk4.jl:44-217 (coherent RK4
-  step, jump probabilities from compressed jump MPOs, jump selection, measurements)
+  step, jump probabilities from compressed jump MPOs, jump selection, measurements); with
+  order=1, examples/spin_model_quantum_trajectory.jl:42-190 (coherent step
+  compress_var_apply_H!(A_coh, envop, A, A, expH, 1) with expH = 1 - i dt H)
 * ``run_density``     examples/spin_model_density_matrix.jl:36-203 (in-place RK4 of vec(rho),
   trace / population measurements)
 
@@ -34,7 +36,7 @@ def uniforms(seed, nsteps):
     return g.random(nsteps), g.random(nsteps)
 
 
-def run_trajectory(p, dmax, dt, nsteps, r1, r2, measure_int=10):
+def run_trajectory(p, dmax, dt, nsteps, r1, r2, measure_int=10, order=4):
     """One quantum trajectory; returns a dict of records (jumps, p_coh, e_pop, I_r, final MPS)."""
     na = p.na
     A, dims = R.mpsgroundstate(na, dmax, 2)
@@ -49,13 +51,18 @@ def run_trajectory(p, dmax, dt, nsteps, r1, r2, measure_int=10):
     H2 = M.sm_hamiltonian(p, 0, 1, t[0] + dt / 2)
     H3 = M.sm_hamiltonian(p, 1, dt / 2, t[1])
     H = [H1, H2, H3]
+    expH = M.sm_hamiltonian(p, 1, dt, t[0])
     rec = {"p_coh": np.zeros(nsteps), "jumps": [], "e_pop": [M_measure(A)],
            "I_r": [R.scal_op_prod(A, ir_mpo, A)], "dims": dims}
     for i in range(nsteps):
-        M.update_h(H1, p, 1, dt / 2, t[i])
-        M.update_h(H2, p, 0, 1, t[i] + dt / 2)
-        M.update_h(H3, p, 1, dt / 2, t[i + 1])
-        R.RK4stp_apply_H_half_(dt, H, A_coh, A, A1, A2, A3, env1, env2, env3, envop)
+        if order == 1:
+            M.update_h(expH, p, 1, dt, t[i])
+            R.compress_var_apply_H_(A_coh, envop, A, A, expH, 1)
+        else:
+            M.update_h(H1, p, 1, dt / 2, t[i])
+            M.update_h(H2, p, 0, 1, t[i] + dt / 2)
+            M.update_h(H3, p, 1, dt / 2, t[i + 1])
+            R.RK4stp_apply_H_half_(dt, H, A_coh, A, A1, A2, A3, env1, env2, env3, envop)
         p_coh = R.normalize_lo_(A_coh)
         rec["p_coh"][i] = p_coh
         if r1[i] < p_coh:

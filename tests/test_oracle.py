@@ -430,3 +430,16 @@ def test_two_site_rk4_step_is_the_dense_rk4_map_at_full_bond_dimension():
         want = D.rk4_dense_step(*Hd, want, dt)
         assert np.linalg.norm(D.mps_to_dense(psi) - want) < 1e-11 * np.linalg.norm(want)
     assert dd == [1, 2, 4, 8, 4, 2, 1]
+
+
+def test_first_order_trajectory_step_agrees_with_rk4_to_second_order():
+    """examples/spin_model_quantum_trajectory.jl (coherent step 1 - i dt H_eff through
+    compress_var_apply_H!) against the RK4 example: the no-jump probabilities of the first
+    steps agree to O(dt^2)."""
+    from oracle import drivers as ODR
+    p = M.SpinChain(8, omega=0.5)
+    r1, r2 = np.zeros(3), np.zeros(3)            # no jumps
+    a = ODR.run_trajectory(p, 16, 0.01, 3, r1, r2, measure_int=1, order=1)
+    b = ODR.run_trajectory(p, 16, 0.01, 3, r1, r2, measure_int=1, order=4)
+    assert np.all(np.abs(a["p_coh"] - b["p_coh"]) < 1e-3)
+    assert np.abs(a["p_coh"] - b["p_coh"]).max() > 1e-6    # the first-order step is not unitary to O(dt^2)
