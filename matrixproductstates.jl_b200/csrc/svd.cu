@@ -519,7 +519,9 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
     for (int j = na - 2; j >= 0; --j) {
       MPSB_TRY(pair(j));
       MPSB_TRY(svd_pair(j, k));
-      dnew = truncation_rule(S, k, svd_tol, dlim);
+      // the scratch holds bond j+1 up to cap[j+1], which bounds the rule's result whenever the
+      // guess obeys the dims rule; a guess with larger bonds is clamped here, never overrun
+      dnew = std::min<int>(truncation_rule(S, k, svd_tol, dlim), (int)cap[j + 1]);
       if (dnew == 0) { set_last_message("two-site compression: zero pair tensor"); return MPSB_ERR_NONFINITE; }
       dims[j + 1] = dnew;
       const int n = d * (int)dims[j + 2];
@@ -534,7 +536,9 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
     for (int j = 0; j <= na - 2; ++j) {
       MPSB_TRY(pair(j));
       MPSB_TRY(svd_pair(j, k));
-      dnew = truncation_rule(S, k, svd_tol, dlim);
+      // the scratch holds bond j+1 up to cap[j+1], which bounds the rule's result whenever the
+      // guess obeys the dims rule; a guess with larger bonds is clamped here, never overrun
+      dnew = std::min<int>(truncation_rule(S, k, svd_tol, dlim), (int)cap[j + 1]);
       if (dnew == 0) { set_last_message("two-site compression: zero pair tensor"); return MPSB_ERR_NONFINITE; }
       dims[j + 1] = dnew;
       const int m = (int)dims[j] * d;
