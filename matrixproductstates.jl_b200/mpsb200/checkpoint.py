@@ -2,13 +2,14 @@
 examples/rydberg_pollution_density_matrix_gpu_restart.jl:151-189, writer `write_data_file`
 :238-266).
 
-No MAT-file library is available, so the container is NumPy's ``.npz`` (a zip of ``.npy``
-arrays, readable without this package).  Field names follow the reference writer: scalars
-and arrays are stored as they are; an MPS (a device ``MPS`` or a list of host site arrays,
-the reference's ``collect.(rho)``) is stored site by site as ``<name>/<k>`` (column-major
-``[chiL, d, chiR]`` complex128) and restored as a device ``MPS`` (or host sites).  A write
-goes to ``<file>.tmp`` first and is renamed into place, so an interrupted write never
-replaces the previous checkpoint.
+Two containers, chosen by the file name.  ``*.mat``: a MAT v5 file (scipy.io), readable by
+MATLAB, MAT.jl and scipy, with the reference writer's variable names; an MPS (a device
+``MPS`` or a list of host site arrays, the reference's ``collect.(rho)``) is a cell array of
+complex ``[chiL, d, chiR]`` sites, as MAT.jl writes a Vector of arrays (the reference's own
+files are MAT v7.3, an HDF5 layout no library here writes).  Anything else: NumPy's ``.npz``
+with each MPS site stored as ``<name>/<k>``.  MPS fields are restored as device ``MPS``
+objects (or host sites).  A write goes to ``<file>.tmp`` first and is renamed into place, so
+an interrupted write never replaces the previous checkpoint.
 """
 import json
 import os
@@ -18,17 +19,27 @@ import numpy as np
 _MPS_KEY = "__mps__"
 
 
+def _mps_sites(v):
+    if hasattr(v, "sites") and hasattr(v, "dims"):          # device MPS
+        return v.sites()
+    if isinstance(v, (list, tuple)) and v and all(isinstance(a, np.ndarray) and a.ndim == 3 for a in v):
+        return list(v)
+    return None
+
+
+def _is_mat(filename):
+    return filename.lower().endswith(".mat")
+
+
 def write_data_file(filename, fields):
     """Write ``fields`` (name -> scalar / array / MPS / list of site arrays) to ``filename``."""
+    if _is_mat(filename):
+        return _write_mat(filename, fields)
     arrays, mps_names = {}, []
     for name, v in fields.items():
         if "/" in name or name == _MPS_KEY:
             raise ValueError("field name %r is reserved" % name)
-        sites = None
-        if hasattr(v, "sites") and hasattr(v, "dims"):          # device MPS
-            sites = v.sites()
-        elif isinstance(v, (list, tuple)) and v and all(isinstance(a, np.ndarray) and a.ndim == 3 for a in v):
-            sites = list(v)
+        sites = _mps_sites(v)
         if sites is not None:
             mps_names.append(name)
             for k, a in enumerate(sites):
@@ -42,10 +53,58 @@ def write_data_file(filename, fields):
     os.replace(tmp, filename)
 
 
+def _write_mat(filename, fields):
+    import scipy.io
+    out = {}
+    for name, v in fields.items():
+        if not name.isidentifier():
+            raise ValueError("field name %r is not a MAT variable name" % name)
+        sites = _mps_sites(v)
+        if sites is not None:
+            cell = np.empty((len(sites), 1), dtype=object)   # a column cell array, as MAT.jl writes
+            for k, a in enumerate(sites):
+                cell[k, 0] = np.asarray(a, dtype=np.complex128)
+            out[name] = cell
+        else:
+            out[name] = np.asarray(v)
+    tmp = filename + ".tmp"
+    with open(tmp, "wb") as f:
+        scipy.io.savemat(f, out, format="5", do_compression=False, oned_as="row")
+    os.replace(tmp, filename)
+
+
+def _read_mat(filename):
+    import scipy.io
+    raw = scipy.io.loadmat(filename, squeeze_me=False, chars_as_strings=True)
+    out, mps = {}, {}
+    for name, a in raw.items():
+        if name.startswith("__"):
+            continue
+        if a.dtype == object:                                  # a cell array: an MPS
+            mps[name] = [np.asarray(c, dtype=np.complex128).reshape(c.shape + (1,) * (3 - c.ndim))
+                         for c in a.ravel(order="F")]
+        elif a.dtype.kind == "U":
+            out[name] = str(a[0]) if a.size else ""
+        else:
+            # 1-d arrays go out as 1 x n rows: a row comes back 1-d, an n x 1 matrix stays 2-d
+            out[name] = a.reshape(()).item() if a.size == 1 else (a.ravel() if a.ndim == 2 and a.shape[0] == 1 else a)
+    return out, mps
+
+
 def read_data_file(filename, ctx=None, device=True):
     """Read a checkpoint.  MPS fields come back as device ``MPS`` objects on ``ctx`` (the
     default context when None) if ``device``, else as lists of host site arrays; 0-d arrays
-    come back as Python scalars."""
+    (1 x 1 in a MAT file) come back as Python scalars, MAT row vectors (how 1-d arrays are
+    written) as 1-d."""
+    if _is_mat(filename):
+        out, mps = _read_mat(filename)
+        for name, sites in mps.items():
+            if device:
+                from .core import MPS
+                out[name] = MPS.from_sites(sites, ctx)
+            else:
+                out[name] = sites
+        return out
     out = {}
     with np.load(filename, allow_pickle=False) as z:
         mps_names = json.loads(bytes(z[_MPS_KEY]).decode())

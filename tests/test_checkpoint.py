@@ -8,11 +8,14 @@ import pytest
 from oracle import mps_ref as R
 
 
-def test_checkpoint_round_trip_host(tmp_path):
+@pytest.mark.parametrize("ext", [".npz", ".mat"])
+def test_checkpoint_round_trip_host(tmp_path, ext):
+    """Both containers: NumPy .npz, and a MAT v5 file with the reference writer's variable
+    names and the MPS as a cell array of complex sites (readable by MATLAB / MAT.jl / scipy)."""
     from mpsb200 import checkpoint as CK
     rng = np.random.default_rng(1)
     sites, dims = R.mpsrandom(6, 8, 4, rng)
-    f = str(tmp_path / "run_temp.npz")
+    f = str(tmp_path / ("run_temp" + ext))
     CK.write_data_file(f, {"rho": sites, "i_last": 17, "dt": 0.005, "tr_rho": np.array([1.0 + 0j, 0.99]),
                            "rj": np.arange(6.0)})
     st = CK.read_data_file(f, device=False)
@@ -22,15 +25,21 @@ def test_checkpoint_round_trip_host(tmp_path):
     assert not os.path.exists(f + ".tmp")
     with pytest.raises(ValueError):
         CK.write_data_file(f, {"a/b": 1})
+    if ext == ".mat":   # what a MAT reader sees: a column cell array of 3-d complex sites
+        import scipy.io
+        raw = scipy.io.loadmat(f)
+        assert raw["rho"].shape == (6, 1) and raw["rho"][2, 0].shape == sites[2].shape
+        assert raw["i_last"].shape == (1, 1)
 
 
 @pytest.mark.gpu
-def test_resumed_density_run_equals_uninterrupted(gpu_ctx, tmp_path):
+@pytest.mark.parametrize("ext", [".npz", ".mat"])
+def test_resumed_density_run_equals_uninterrupted(gpu_ctx, tmp_path, ext):
     from mpsb200 import drivers as GDR, models as GM
     na, chi, dt, n = 6, 16, 0.005, 8
     pg = GM.WaveguideChain(na, gam_eg=0.1, omega=0.5, gam_phi=0.1)
     b_ref, obs_ref = GDR.run_density(pg, chi, dt, n, w=8, measure_int=2, ctx=gpu_ctx)
-    f = str(tmp_path / "rho_temp.npz")
+    f = str(tmp_path / ("rho_temp" + ext))
     GDR.run_density(pg, chi, dt, 4, w=8, measure_int=2, ctx=gpu_ctx, checkpoint=f, checkpoint_int=4)
     b, obs = GDR.run_density(pg, chi, dt, n, w=8, measure_int=2, ctx=gpu_ctx, checkpoint=f)
     assert all(np.array_equal(a, c) for a, c in zip(b.rho.sites(), b_ref.rho.sites()))
