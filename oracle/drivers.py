@@ -118,8 +118,9 @@ def rho_observables(rho, pairs=((1, 2),)):
     return tr, see, spm
 
 
-def run_density(p, dmax, dt, nsteps, w=6, measure_int=10, pairs=((1, 2),), rho=None):
-    """In-place density-matrix RK4 (the 10-argument form) from the all-down product state."""
+def run_density(p, dmax, dt, nsteps, w=6, measure_int=10, pairs=((1, 2),), rho=None, progress=None):
+    """In-place density-matrix RK4 (the 10-argument form) from the all-down product state
+    (or from ``rho``); ``progress(i)``, when given, is called after every step."""
     na = p.na
     if rho is None:
         rho, dims = R.mpsgroundstate(na, dmax, 4)
@@ -135,6 +136,8 @@ def run_density(p, dmax, dt, nsteps, w=6, measure_int=10, pairs=((1, 2),), rho=N
         R.RK4stp_apply_H_half_(dt, L, rho, rho, rho1, rho2, rho3, env1, env2, env3, envop)
         if (i + 1) % measure_int == 0:
             obs.append(rho_observables(rho, pairs))
+        if progress is not None:
+            progress(i + 1)
     return rho, obs
 
 
