@@ -63,6 +63,17 @@ int mpsb_ctx_set_graphs(mpsb_ctx* ctx, int enable);
  * env1..env3 / envop buffers end up holding other stages' environments than the reference's
  * (they are scratch to every reference caller).  No reference counterpart. */
 int mpsb_ctx_set_pipeline(mpsb_ctx* ctx, int enable);
+/* Contraction precision of the sweep entry points (mpsb_rk4stp_apply_H_half, the
+ * compress_* family).  slices = 0: FP64 (the default, the drop-in path).  slices = 3..7: each
+ * complex GEMM of a sweep whose output spans at least `min_tiles` 128 x 32-complex tiles runs on
+ * the int8 tensor pipe (tcgen05) with both operands written as `slices` 7-bit slices under a
+ * per-row / per-column power-of-two scale, all slice products of equal weight accumulated
+ * exactly in int32 and combined in FP64 (relative accuracy about 2^(-7 slices) of the
+ * operands' row / column maxima); smaller GEMMs, the QR gauge moves, norms, MPO applies and
+ * every observable stay FP64.  The reference computes in the element type of its arrays
+ * (Complex{Float64}, or Complex{Float32} in its GPU examples,
+ * examples/rydberg_density_matrix_gpu.jl:124-125); this setting has no direct counterpart. */
+int mpsb_ctx_set_precision(mpsb_ctx* ctx, int slices, int min_tiles);
 /* Kernel launches issued by this context since creation (for accounting). */
 int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out);
 
@@ -264,6 +275,13 @@ int mpsb_op_svd(mpsb_ctx* ctx, const void* X, void* U, double* S, void* V, int m
 /* Q of the LAPACK geqrf+orgqr QR of the column-major m x n matrix X (m >= n):
  * qrq!(X)  src/orthonormalisation.jl:180-184. Q may alias X. R (n x n) optional (NULL). */
 int mpsb_op_qr(mpsb_ctx* ctx, const void* X, void* Q, void* R, int m, int n);
+/* C = alpha op(A) op(B) + beta C on device buffers with element strides (complex128;
+ * op = conjugate when conjA / conjB), the GEMM every contraction of src/mps_base.jl reduces to
+ * (BLAS zgemm there).  slices = 0: FP64 (DMMA); 3..7: the int8-sliced tensor-core path of
+ * mpsb_ctx_set_precision.  alpha / beta: interleaved complex, NULL = 1 / 0. */
+int mpsb_op_zgemm(mpsb_ctx* ctx, int M, int N, int K, const void* A, int64_t a_m, int64_t a_k, int conjA,
+                  const void* B, int64_t b_k, int64_t b_n, int conjB, void* C, int64_t c_m, int64_t c_n,
+                  const double* alpha, const double* beta, int slices);
 
 #ifdef __cplusplus
 }

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "engine.cuh"
+#include "ozaki.cuh"
 
 namespace mpsb {
 
@@ -41,7 +42,8 @@ static int sync(mpsb_ctx* ctx) {
     *hw = 0;
     cudaMemsetAsync(ctx->err(), 0, sizeof(int), ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    set_last_message("a device-side exchange wait timed out (QR cluster kernel); results of this stream are invalid");
+    set_last_message("a device-side wait timed out (%s); results of this stream are invalid",
+                     (*hw & 2) ? "sliced GEMM pipeline" : "QR cluster exchange");
     return MPSB_ERR_CUDA;
   }
   return MPSB_OK;
@@ -160,15 +162,9 @@ int mpsb_ctx_destroy(mpsb_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto& kv : ctx->graphs_cache)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-  for (auto& b : ctx->ws.named)
-    if (b.p) cudaFree(b.p);
-  if (ctx->ws.splitk.p) cudaFree(ctx->ws.splitk.p);
-  if (ctx->ws.qr.p) cudaFree(ctx->ws.qr.p);
-  if (ctx->ws.svd.p) cudaFree(ctx->ws.svd.p);
   cudaStreamSynchronize(ctx->side);
-  for (auto& b : ctx->ws_side.named)
-    if (b.p) cudaFree(b.p);
-  if (ctx->ws_side.splitk.p) cudaFree(ctx->ws_side.splitk.p);
+  ws_free(ctx->ws);
+  ws_free(ctx->ws_side);
   for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
   cudaFree(ctx->d_scalars);
   cudaFreeHost(ctx->h_scalars);
@@ -201,6 +197,18 @@ int mpsb_ctx_set_graphs(mpsb_ctx* ctx, int enable) {
 int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out) {
   if (!ctx || !out) return MPSB_ERR_INVALID_ARG;
   *out = ctx->ws.launches + ctx->ws_side.launches;
+  return MPSB_OK;
+}
+
+int mpsb_ctx_set_precision(mpsb_ctx* ctx, int slices, int min_tiles) {
+  if (!ctx) return MPSB_ERR_INVALID_ARG;
+  if (slices != 0 && (slices < OZ_MIN_SLICES || slices > OZ_MAX_SLICES)) {
+    set_last_message("precision: slices must be 0 (FP64) or %d..%d", OZ_MIN_SLICES, OZ_MAX_SLICES);
+    return MPSB_ERR_INVALID_ARG;
+  }
+  if (min_tiles < 1) return MPSB_ERR_INVALID_ARG;
+  ctx->split_slices = slices;
+  ctx->split_min_tiles = min_tiles;
   return MPSB_OK;
 }
 
@@ -720,6 +728,29 @@ int mpsb_op_svd(mpsb_ctx* ctx, const void* X, void* U, double* S, void* V, int m
   if (ctx->ws.svd.p != before) ctx->ws_generation++;
   MPSB_TRY(st);
   return sync(ctx);
+}
+
+int mpsb_op_zgemm(mpsb_ctx* ctx, int M, int N, int K, const void* A, int64_t a_m, int64_t a_k, int conjA,
+                  const void* B, int64_t b_k, int64_t b_n, int conjB, void* C, int64_t c_m, int64_t c_n,
+                  const double* alpha, const double* beta, int slices) {
+  MPSB_TRY(bind(ctx));
+  if (!A || !B || !C || M < 1 || N < 1 || K < 0) return MPSB_ERR_DIMENSION;
+  Gemm g;
+  g.M = M; g.N = N; g.K = K;
+  g.A = DP(A); g.a_m = a_m; g.a_k = a_k; g.conjA = conjA != 0;
+  g.B = DP(B); g.b_k = b_k; g.b_n = b_n; g.conjB = conjB != 0;
+  g.C = DW(C); g.c_m = c_m; g.c_n = c_n;
+  if (alpha) g.alpha = cmk(alpha[0], alpha[1]);
+  if (beta) g.beta = cmk(beta[0], beta[1]);
+  if (slices == 0) return run_gemm(ctx, g);
+  if (!ozgemm_supported(g, slices)) {
+    set_last_message("zgemm: %d slices unsupported for M=%d N=%d K=%d", slices, M, N, K);
+    return MPSB_ERR_UNSUPPORTED;
+  }
+  void* before = ctx->ws.oz.p;
+  MPSB_TRY(devbuf_ensure(&ctx->ws, ctx->ws.oz, ozgemm_scratch_bytes(g, slices)));
+  if (ctx->ws.oz.p != before) ctx->ws_generation++;
+  return ozgemm_launch(g, slices, ctx->ws.oz.p, ctx->ws.oz.cap, ctx->err(), &ctx->ws, ctx->stream);
 }
 
 int mpsb_op_qr(mpsb_ctx* ctx, const void* X, void* Q, void* R, int m, int n) {

@@ -63,6 +63,11 @@ __host__ __device__ __forceinline__ cd crecip(cd z) {
 void set_last_error(cudaError_t e, const char* what, const char* file, int line);
 void set_last_message(const char* fmt, ...);
 
+// Kernel attributes are per device: set the dynamic shared-memory limit of kernel `fn` (and,
+// when `cluster16`, permission for non-portable cluster sizes) once per (kernel, current device)
+// in this process; thread-safe.
+int ensure_kernel_attrs(const void* fn, int smem_bytes, bool cluster16 = false);
+
 // ---------------------------------------------------------------------------------
 // Strided complex GEMM descriptor: C[m,n] = alpha * sum_k opA[m,k] opB[k,n] + beta * C[m,n]
 // for b in [0, batch).  Every operand is addressed by element strides, so transposes and

@@ -5,8 +5,18 @@
 #include <cstring>
 
 #include "engine.cuh"
+#include "ozaki.cuh"
 
 namespace mpsb {
+
+// While alive, the sweep contractions of this context run at its configured precision
+// (mpsb_ctx_set_precision); outside (observables, gauge moves, eigen-solvers) they are FP64.
+struct SplitScope {
+  mpsb_ctx* c;
+  bool prev;
+  explicit SplitScope(mpsb_ctx* ctx) : c(ctx), prev(ctx->split_on) { c->split_on = c->split_slices > 0; }
+  ~SplitScope() { c->split_on = prev; }
+};
 
 int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out) {
   DevBuf& b = ctx->ws.named[s];
@@ -17,7 +27,18 @@ int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out) {
   return MPSB_OK;
 }
 
+static bool split_worth(const mpsb_ctx* ctx, const Gemm& g) {
+  const int64_t tiles = ((int64_t)(g.M + 127) / 128) * ((2 * (int64_t)g.N + 63) / 64);
+  return tiles >= ctx->split_min_tiles && g.K >= 16;
+}
+
 int run_gemm(mpsb_ctx* ctx, const Gemm& g) {
+  if (ctx->split_on && ozgemm_supported(g, ctx->split_slices) && split_worth(ctx, g)) {
+    void* before_oz = ctx->ws.oz.p;
+    MPSB_TRY(devbuf_ensure(&ctx->ws, ctx->ws.oz, ozgemm_scratch_bytes(g, ctx->split_slices)));
+    if (ctx->ws.oz.p != before_oz) ctx->ws_generation++;
+    return ozgemm_launch(g, ctx->split_slices, ctx->ws.oz.p, ctx->ws.oz.cap, ctx->err(), &ctx->ws, ctx->stream);
+  }
   void* before = ctx->ws.splitk.p;
   int st = gemm_launch(g, &ctx->ws, ctx->stream);
   if (ctx->ws.splitk.p != before) ctx->ws_generation++;
@@ -356,6 +377,7 @@ int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* 
                              const mpsb_mpo* H) {
   if (!ctx || !A0 || !envop || !Ain || !coef || !A || !H || numv < 1) return MPSB_ERR_INVALID_ARG;
   MPSB_TRY(sum_var_check(A0, env, envop, Ain, numv, A, H));
+  SplitScope scope(ctx);
   SweepScratch s;
   MPSB_TRY(sweep_scratch(ctx, A0, H, numv - 1, s));
   MPSB_TRY(sum_var_init(ctx, right, env, envop, Ain, coef, numv, A, H, s, nullptr));
@@ -374,6 +396,7 @@ int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mps
                          const mpsb_mpo* H, int maxsweeps) {
   if (!ctx || !A0 || !envop || !Ain || !A || !H || maxsweeps < 0) return MPSB_ERR_INVALID_ARG;
   if (!same_dims(A0, Ain) || !same_dims(A0, A) || !envop->three || H->na != A0->na) return MPSB_ERR_DIMENSION;
+  SplitScope scope(ctx);
   const int na = A0->na, d = A0->d;
   for (int k = 0; k <= na; ++k)
     if (envop->d1[k] != A0->dims[k] || envop->d2[k] != A0->dims[k] || envop->w[k] != H->w[k]) return MPSB_ERR_DIMENSION;
@@ -415,6 +438,7 @@ int compress_sum_var_full(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const cd
                           const mpsb_mps* const* A, const mpsb_mpo* H, int maxsweeps) {
   if (!ctx || !A0 || !coef || !A || numv < 1 || maxsweeps < 0) return MPSB_ERR_INVALID_ARG;
   const bool hasH = H != nullptr;
+  SplitScope scope(ctx);
   if (hasH && !envop) return MPSB_ERR_INVALID_ARG;
   const int np = hasH ? numv - 1 : numv;
   if (np < 1) {   // the reference indexes the first plain term unconditionally
@@ -652,11 +676,12 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
              mpsb_env* env3, mpsb_env* envop) {
   if (!ctx || !H1 || !H2 || !H3 || !psi0 || !psi || !psi1 || !psi2 || !psi3 || !env1 || !env2 || !env3 || !envop)
     return MPSB_ERR_INVALID_ARG;
+  SplitScope scope(ctx);
   if (!ctx->graphs)
     return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
   int64_t dtbits;
   std::memcpy(&dtbits, &dt, sizeof(dt));
-  std::vector<int64_t> key = {ctx->pipeline ? 2 : 1, dtbits, H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial,
+  std::vector<int64_t> key = {ctx->pipeline ? 2 : 1, ctx->split_slices, ctx->split_min_tiles, dtbits, H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial,
                               psi1->serial, psi2->serial, psi3->serial, env1->serial, env2->serial,
                               env3->serial, envop->serial};
   auto& ent = ctx->graphs_cache[key];

@@ -21,10 +21,16 @@ struct mpsb_ctx {
   std::vector<cudaEvent_t> events;   // per-site / fork / join events, created on first use
   bool pipeline = true;
   bool graphs = true;
+  // contraction precision of the sweeps: 0 = FP64 (DMMA); 3..7 = int8-sliced tensor-core GEMM
+  // with that many slices per operand, used for GEMMs of at least split_min_tiles output tiles
+  int split_slices = 0;
+  int split_min_tiles = 64;
+  bool split_on = false;       // set while a sweep entry point issues its contractions
   int64_t ws_generation = 0;   // bumped whenever a scratch buffer is reallocated
   double* d_scalars = nullptr; // small device scratch for norms (64 doubles)
   double* h_scalars = nullptr; // pinned host mirror
-  // device error word (inside d_scalars[63]): kernels whose bounded waits run out set bit 0
+  // device error word (inside d_scalars[63]): kernels whose bounded waits run out set a bit
+  // (bit 0: the QR cluster's exchanges, bit 1: the sliced GEMM's pipeline)
   int* err() const { return reinterpret_cast<int*>(d_scalars + 63); }
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;

@@ -288,12 +288,7 @@ int gemm_launch(const Gemm& g, Workspace* ws, cudaStream_t s) {
     MPSB_TRY(ws_splitk(ws, bytes, &P.ws));
   }
   KernelFn fn = pick(g);
-  static bool attr_done[16] = {false};
-  int key = (g.conjA ? 8 : 0) | (g.conjB ? 4 : 0) | (g.a_m == 1 ? 2 : 0) | (g.b_k == 1 ? 1 : 0);
-  if (!attr_done[key]) {
-    MPSB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
-    attr_done[key] = true;
-  }
+  MPSB_TRY(ensure_kernel_attrs((const void*)fn, (int)SMEM_BYTES));
   dim3 grid(tiles, splits, g.batch);
   fn<<<grid, NT, SMEM_BYTES, s>>>(P);
   MPSB_CUDA_TRY(cudaGetLastError());

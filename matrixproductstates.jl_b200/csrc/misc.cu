@@ -1,8 +1,25 @@
 // Small kernels of the sweeps: boundary-env writes, FP64 norms, rescaling, local_exp.
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "common.cuh"
 #include "misc.cuh"
 
 namespace mpsb {
+
+int ensure_kernel_attrs(const void* fn, int smem_bytes, bool cluster16) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  MPSB_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, fn})) return MPSB_OK;
+  MPSB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
+  if (cluster16) MPSB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  done.insert({dev, fn});
+  return MPSB_OK;
+}
 namespace {
 
 __global__ void set_value_kernel(cd* p, cd v) { *p = v; }

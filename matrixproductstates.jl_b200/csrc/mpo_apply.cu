@@ -86,11 +86,7 @@ int mpo_apply_launch_strided(const MpoApply& a, int64_t op_k1, int64_t op_k2, in
   size_t smem = (size_t)(K * M + K * TX) * sizeof(cd);
   if (smem > 200 * 1024) return MPSB_ERR_UNSUPPORTED;
   if (a.Y > 65535) return MPSB_ERR_UNSUPPORTED;
-  static bool attr = false;
-  if (!attr) {
-    MPSB_CUDA_TRY(cudaFuncSetAttribute(mpo_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr = true;
-  }
+  MPSB_TRY(ensure_kernel_attrs((const void*)mpo_apply_kernel, 200 * 1024));
   MpoParams P;
   P.a = a;
   P.op_k1 = op_k1; P.op_k2 = op_k2; P.op_m1 = op_m1; P.op_m2 = op_m2;

@@ -1,0 +1,552 @@
+// Split-precision complex GEMM on the 5th-generation tensor cores (tcgen05, kind::i8).
+//
+// The environment and effective-operator contractions of src/mps_base.jl (prod_AOR's first
+// GEMM, prod_AOL's first GEMM, prod_LR!, update_re!, update_le!, update_renv!, update_lenv!)
+// are complex128 GEMMs C = alpha op(A) op(B) + beta C.  tcgen05 has no FP64 kind, so this path
+// writes each FP64 operand as a sum of S integer slices and multiplies the slices on the int8
+// tensor pipe, where products accumulate exactly in int32 (the Ozaki scheme):
+//
+//   * complex -> real: C' (M x 2N) = A' (M x 2K) B' (2K x 2N) with A' rows the interleaved
+//     (re, im) pairs of A's rows and B' column pairs (n,re) = [re, -im ...], (n,im) = [im, re ...]
+//     of B's columns, so one real GEMM gives both components;
+//   * each row r of A' (column of B') gets an exponent E_r with |x| < 2^E_r, and the scaled row
+//     x 2^(7-E_r) is peeled into digits d_0..d_{S-1} in [-127, 127] with
+//     x = 2^E_r sum_i 2^(-7(i+1)) d_i + O(2^(E_r - 7S))   (exact FP64 arithmetic);
+//   * level t = i + j collects every slice product A_i B_j of the same weight 2^(-7(t+2)) in one
+//     int32 TMEM accumulator (exact: |sum| <= S * 127^2 * 2K < 2^31 for 2K < 2^17 / S);
+//     levels t < S are kept (S(S+1)/2 MMAs per k-step), the rest are the truncation;
+//   * the epilogue reads the S accumulators, sums them in FP64 from the smallest weight up,
+//     applies 2^(E_a + E_b), alpha and beta, and writes complex128 C through its strides.
+//
+// Kernel (one 128 x 64 tile of C' per CTA, 256 threads): warp 0 issues TMA loads of the 2S
+// slice tiles of each 64-byte k-stage (64B swizzle) into a shared-memory ring, warp 1 owns the
+// TMEM allocation and one lane issues tcgen05.mma for all slice pairs of a stage and commits
+// the stage back to the producer, warps 4..7 are the epilogue (TMEM lanes 0..127).  Every wait
+// is bounded in wall-clock time: a wait that runs out sets the context's error word and the CTA
+// winds down (copies in flight land, the TMEM allocation is released).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "common.cuh"
+#include "ozaki.cuh"
+#include "workspace.cuh"
+
+namespace mpsb {
+
+namespace {
+
+constexpr int OZ_BM = 128;        // rows of A' per tile (tcgen05 M)
+constexpr int OZ_BN = 64;         // columns of C' per tile (tcgen05 N): 32 complex columns
+constexpr int OZ_BK = 64;         // int8 k per stage: one 64-byte swizzled row
+constexpr int OZ_KP_ALIGN = 64;   // K' padding
+constexpr int A_TILE = OZ_BM * OZ_BK;   // 8 KB
+constexpr int B_TILE = OZ_BN * OZ_BK;   // 4 KB
+constexpr int OZ_THREADS = 256;
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // a bounded mbarrier wait gives up after 2 s
+
+__host__ __device__ constexpr int stage_bytes(int S) { return S * (A_TILE + B_TILE); }
+__host__ __device__ constexpr int num_stages(int S) {
+  return (220 * 1024) / stage_bytes(S) > 4 ? 4 : (220 * 1024) / stage_bytes(S);
+}
+__host__ __device__ constexpr int tmem_cols(int S) { return S * OZ_BN <= 256 ? 256 : 512; }
+__host__ __device__ constexpr int smem_bytes(int S) { return 1024 + num_stages(S) * stage_bytes(S) + 256; }
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// non-blocking test of the phase of the given parity
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// wait for the phase of the given parity, bounded in wall-clock time; false when it ran out
+__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_test(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned i = 1;; ++i) {
+    if (mbar_test(bar, parity)) return true;
+    if ((i & 255) == 0 && global_ns() - t0 > WAIT_NS) return false;
+    __nanosleep(32);
+  }
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];\n" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+// K-major operand with 64-byte swizzle: rows of 64 bytes, 8-row groups 512 bytes apart
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);        // start address
+  d |= (uint64_t)1 << 16;                        // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;               // stride byte offset: 8 rows x 64 B
+  d |= (uint64_t)1 << 46;                        // descriptor version (sm_100)
+  d |= (uint64_t)4 << 61;                        // layout: 64-byte swizzle
+  return d;
+}
+// instruction descriptor: kind::i8, signed A and B, s32 accumulator, both K-major, M=128, N=64
+__host__ __device__ constexpr uint32_t idesc_i8() {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+}
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc_i8()), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------- slicing
+// A view of the operand whose rows become rows of the sliced matrix: element (r, k) at
+// X[r * x_r + k * x_k], conjugated when conj.  In B mode a row (a column n of op(B)) becomes
+// the pair of rows (n,re) = [re, -im], (n,im) = [im, re] of B'^T; otherwise a row is [re, im].
+struct SliceView {
+  const cd* X; int R, K; int64_t x_r, x_k; bool conj;
+};
+
+// biased IEEE exponent of max(|re|, |im|) (0 for zero / subnormal), max-reduced per row into
+// rexp (zeroed before)
+__global__ void oz_rowexp_kernel(SliceView v, int* __restrict__ rexp) {
+  __shared__ int tile_e[32][33];
+  const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int tid = threadIdx.x;
+  const bool rc = (v.x_r == 1);   // rows contiguous: lanes run along r
+  for (int i = 0; i < 4; ++i) {
+    int rr, kk;
+    if (rc) { rr = tid % 32; kk = tid / 32 + 8 * i; }
+    else    { kk = tid % 32; rr = tid / 32 + 8 * i; }
+    const int r = r0 + rr, k = k0 + kk;
+    int e = 0;
+    if (r < v.R && k < v.K) {
+      const cd x = v.X[(int64_t)r * v.x_r + (int64_t)k * v.x_k];
+      const double m = fmax(fabs(x.x), fabs(x.y));
+      e = (int)((__double_as_longlong(m) >> 52) & 0x7FF);
+    }
+    tile_e[rr][kk] = e;
+  }
+  __syncthreads();
+  const int warp = tid / 32, lane = tid % 32;
+  for (int rr = warp; rr < 32; rr += 8) {
+    int e = tile_e[rr][lane];
+    for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+    if (lane == 0 && e > 0 && r0 + rr < v.R) atomicMax(rexp + r0 + rr, e);
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void digits(double x, int E, int (&d)[S]) {
+  // x 2^(7-e) in (-128, 128) with e the frexp exponent of the row maximum; every step below is
+  // exact in FP64
+  double t = (E > 0) ? ldexp(x, 7 - (E - 1022)) : 0.0;
+#pragma unroll
+  for (int i = 0; i < S; ++i) {
+    const double q = fmin(fmax(rint(t), -127.0), 127.0);
+    d[i] = (int)q;
+    t = (t - q) * 128.0;
+  }
+}
+
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+  return (uint32_t)(uint8_t)a | ((uint32_t)(uint8_t)b << 8) | ((uint32_t)(uint8_t)c << 16) |
+         ((uint32_t)(uint8_t)d << 24);
+}
+
+// Digits of a 32-row x 32-complex tile: out[t][row][k'] (K' = 2K padded to Kp, rows padded to
+// the tile grid with zeros, so every byte the GEMM reads is written).
+template <int S, bool BMODE>
+__global__ void oz_split_kernel(SliceView v, const int* __restrict__ rexp, int8_t* __restrict__ out, int64_t rows_out,
+                                int Kp) {
+  __shared__ cd tile[32][33];
+  const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int tid = threadIdx.x;
+  const bool rc = (v.x_r == 1);
+  for (int i = 0; i < 4; ++i) {
+    int rr, kk;
+    if (rc) { rr = tid % 32; kk = tid / 32 + 8 * i; }
+    else    { kk = tid % 32; rr = tid / 32 + 8 * i; }
+    const int r = r0 + rr, k = k0 + kk;
+    cd x = cmk(0.0, 0.0);
+    if (r < v.R && k < v.K) {
+      x = v.X[(int64_t)r * v.x_r + (int64_t)k * v.x_k];
+      if (v.conj) x.y = -x.y;
+    }
+    tile[rr][kk] = x;
+  }
+  __syncthreads();
+  // thread -> (row, 4 consecutive complex k)
+  const int rr = tid / 8, kq = (tid % 8) * 4;
+  const int r = r0 + rr;
+  const int E = (r < v.R) ? rexp[r] : 0;
+  int dre[4][S], dim[4][S];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const cd x = tile[rr][kq + j];
+    digits<S>(x.x, E, dre[j]);
+    digits<S>(x.y, E, dim[j]);
+  }
+  const int64_t kbyte = 2 * (int64_t)(k0 + kq);   // first k' of this thread (8 bytes, < Kp)
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    if (!BMODE) {   // row r: [re_k, im_k] pairs
+      int8_t* p = out + ((int64_t)t * rows_out + r) * Kp + kbyte;
+      *reinterpret_cast<uint2*>(p) = make_uint2(pack4(dre[0][t], dim[0][t], dre[1][t], dim[1][t]),
+                                                pack4(dre[2][t], dim[2][t], dre[3][t], dim[3][t]));
+    } else {        // rows 2r (n,re) = [re, -im] and 2r+1 (n,im) = [im, re]
+      int8_t* p = out + ((int64_t)t * rows_out + 2 * (int64_t)r) * Kp + kbyte;
+      *reinterpret_cast<uint2*>(p) = make_uint2(pack4(dre[0][t], -dim[0][t], dre[1][t], -dim[1][t]),
+                                                pack4(dre[2][t], -dim[2][t], dre[3][t], -dim[3][t]));
+      *reinterpret_cast<uint2*>(p + Kp) = make_uint2(pack4(dim[0][t], dre[0][t], dim[1][t], dre[1][t]),
+                                                     pack4(dim[2][t], dre[2][t], dim[3][t], dre[3][t]));
+    }
+  }
+}
+
+// ---------------------------------------------------------------- the tensor-core GEMM
+struct OzParams {
+  int M, N;              // complex extents of C
+  int Mpad, NBpad;       // rows of one A' slice / one B'^T slice in the slice buffers
+  int kstages;           // K' / OZ_BK
+  const int* ea;         // biased exponents per row of A (Mpad)
+  const int* eb;         // biased exponents per complex column of B (NBpad / 2)
+  cd* C; int64_t c_m, c_n;
+  cd alpha, beta;
+  int* err;              // device error word (bit 1: a wait in this kernel ran out)
+};
+
+template <int S>
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+    ozgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzParams P) {
+  constexpr int ST = num_stages(S);
+  constexpr int SB = stage_bytes(S);
+  constexpr int NCOL = tmem_cols(S);
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * SB);
+  uint64_t* empty = full + ST;
+  uint64_t* accum = empty + ST;
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(accum + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int tiles_m = P.Mpad / OZ_BM;
+  const int m_tile = blockIdx.x % tiles_m, n_tile = blockIdx.x / tiles_m;
+  const int m0 = m_tile * OZ_BM, n0 = n_tile * OZ_BN;   // n0 in real columns of C'
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(accum, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_holder)),
+                 "r"(NCOL));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_holder;
+
+  if (warp == 0) {
+    // ---- TMA producer
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+      asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+      int issued = 0;
+      for (int kb = 0; kb < P.kstages; ++kb) {
+        const int s = kb % ST;
+        const uint32_t ph = (kb / ST) & 1;
+        if (!mbar_wait(empty + s, ph ^ 1) || *abort_flag) {
+          *abort_flag = 1;
+          break;
+        }
+        unsigned char* st = smem + s * SB;
+        mbar_expect_tx(full + s, SB);
+#pragma unroll
+        for (int i = 0; i < S; ++i) tma_load_2d(st + i * A_TILE, &tmA, full + s, kb * OZ_BK, i * P.Mpad + m0);
+#pragma unroll
+        for (int j = 0; j < S; ++j)
+          tma_load_2d(st + S * A_TILE + j * B_TILE, &tmB, full + s, kb * OZ_BK, j * P.NBpad + n0);
+        issued = kb + 1;
+      }
+      if (*abort_flag) {
+        // let the copies already in flight land before the CTA goes away
+        for (int kb = (issued > ST ? issued - ST : 0); kb < issued; ++kb) mbar_wait(full + kb % ST, (kb / ST) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    // ---- MMA issuer
+    if (lane == 0) {
+      for (int kb = 0; kb < P.kstages; ++kb) {
+        const int s = kb % ST;
+        const uint32_t ph = (kb / ST) & 1;
+        if (!mbar_wait(full + s, ph) || *abort_flag) {
+          *abort_flag = 1;
+          break;
+        }
+        fence_after();
+        const uint32_t st = smem_u32(smem + s * SB);
+#pragma unroll
+        for (int kk = 0; kk < OZ_BK / 32; ++kk) {
+#pragma unroll
+          for (int i = 0; i < S; ++i) {
+            const uint64_t ad = smem_desc_sw64(st + i * A_TILE + kk * 32);
+#pragma unroll
+            for (int j = 0; j < S - i; ++j) {
+              const uint64_t bd = smem_desc_sw64(st + S * A_TILE + j * B_TILE + kk * 32);
+              const uint32_t acc = (kb > 0 || kk > 0 || i > 0) ? 1u : 0u;   // i == 0 opens every level
+              mma_i8(tmem + (uint32_t)((i + j) * OZ_BN), ad, bd, acc);
+            }
+          }
+        }
+        mma_commit(empty + s);   // the stage's smem is free once these MMAs have read it
+      }
+      mma_commit(accum);         // every MMA of this CTA done (also on the abort path)
+    }
+  } else if (warp >= 4) {
+    // ---- epilogue: TMEM lanes 32*(warp-4) .. +31 are rows m0 + 32*(warp-4) + lane
+    bool ok = true;
+    if (lane == 0) ok = mbar_wait(accum, 0);   // one poller per warp
+    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    fence_after();
+    if (!ok) *abort_flag = 1;
+    const int row = 32 * (warp - 4) + lane;
+    const int m = m0 + row;
+    const uint32_t tbase = tmem + ((uint32_t)(32 * (warp - 4)) << 16);
+    const int Ea = P.ea[m];
+    const bool use_beta = (P.beta.x != 0.0) || (P.beta.y != 0.0);
+    const bool good = ok && !*abort_flag;
+#pragma unroll 1
+    for (int half = 0; half < OZ_BN / 32; ++half) {
+      double acc[32];
+#pragma unroll
+      for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+#pragma unroll
+      for (int t = S - 1; t >= 0; --t) {
+        int v[32];
+        __syncwarp();   // tcgen05.ld is warp-collective
+        tmem_ld32(tbase + (uint32_t)(t * OZ_BN + half * 32), v);
+        const double w = ldexp(1.0, -7 * (t + 2));
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc[c] += (double)v[c] * w;
+      }
+      if (good && m < P.M) {
+        const int nbase = (n0 + half * 32) / 2;   // first complex column of this half
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          const int n = nbase + c;
+          if (n < P.N) {
+            const int Eb = P.eb[n];
+            double re = 0.0, im = 0.0;
+            if (Ea > 0 && Eb > 0) {
+              const int e = (Ea - 1022) + (Eb - 1022);
+              re = ldexp(acc[2 * c], e);
+              im = ldexp(acc[2 * c + 1], e);
+            }
+            cd* cp = P.C + (int64_t)m * P.c_m + (int64_t)n * P.c_n;
+            cd val = cmul(P.alpha, cmk(re, im));
+            if (use_beta) val = cadd(val, cmul(P.beta, *cp));
+            *cp = val;
+          }
+        }
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (*abort_flag && threadIdx.x == 0 && P.err) atomicOr(P.err, 2);
+  if (warp == 1) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(NCOL));
+  }
+}
+
+// ---------------------------------------------------------------- host side
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+
+int get_encoder() {
+  std::call_once(g_encode_once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!g_encode) {
+    set_last_message("cuTensorMapEncodeTiled is not available from the driver");
+    return MPSB_ERR_CUDA;
+  }
+  return MPSB_OK;
+}
+
+// 2-d int8 tensor map of a slice buffer (rows of kp bytes), tiles of 64 bytes x box_rows
+int make_map(CUtensorMap* map, const int8_t* base, int64_t kp, int64_t rows, int box_rows) {
+  cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kp};
+  cuuint32_t box[2] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_message("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return MPSB_ERR_CUDA;
+  }
+  return MPSB_OK;
+}
+
+typedef void (*OzKernel)(CUtensorMap, CUtensorMap, OzParams);
+typedef void (*SplitKernel)(SliceView, const int*, int8_t*, int64_t, int);
+
+template <int S>
+struct OzTable {
+  static OzKernel gemm() { return ozgemm_kernel<S>; }
+  static SplitKernel split(bool b) { return b ? oz_split_kernel<S, true> : oz_split_kernel<S, false>; }
+  static int smem() { return smem_bytes(S); }
+};
+
+OzKernel pick_gemm(int S) {
+  switch (S) {
+    case 3: return OzTable<3>::gemm();
+    case 4: return OzTable<4>::gemm();
+    case 5: return OzTable<5>::gemm();
+    case 6: return OzTable<6>::gemm();
+    case 7: return OzTable<7>::gemm();
+  }
+  return nullptr;
+}
+SplitKernel pick_split(int S, bool b) {
+  switch (S) {
+    case 3: return OzTable<3>::split(b);
+    case 4: return OzTable<4>::split(b);
+    case 5: return OzTable<5>::split(b);
+    case 6: return OzTable<6>::split(b);
+    case 7: return OzTable<7>::split(b);
+  }
+  return nullptr;
+}
+int smem_of(int S) {
+  switch (S) {
+    case 3: return OzTable<3>::smem();
+    case 4: return OzTable<4>::smem();
+    case 5: return OzTable<5>::smem();
+    case 6: return OzTable<6>::smem();
+    case 7: return OzTable<7>::smem();
+  }
+  return 0;
+}
+
+inline int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+bool ozgemm_supported(const Gemm& g, int slices) {
+  if (slices < OZ_MIN_SLICES || slices > OZ_MAX_SLICES) return false;
+  if (g.batch != 1 || g.M <= 0 || g.N <= 0 || g.K <= 0) return false;
+  // exact int32 accumulation: S * 127^2 * 2K < 2^31
+  return (int64_t)slices * 127 * 127 * 2 * (int64_t)g.K < (int64_t(1) << 31);
+}
+
+size_t ozgemm_scratch_bytes(const Gemm& g, int slices) {
+  const int64_t Mpad = round_up(g.M, OZ_BM), NBpad = round_up(2 * (int64_t)g.N, OZ_BN);
+  const int64_t Kp = round_up(2 * (int64_t)g.K, OZ_KP_ALIGN);
+  return (size_t)slices * (Mpad + NBpad) * Kp + (size_t)(Mpad + NBpad / 2) * sizeof(int) + 1024;
+}
+
+int ozgemm_launch(const Gemm& g, int slices, void* scratch, size_t scratch_bytes, int* err, Workspace* ws,
+                  cudaStream_t s) {
+  if (!ozgemm_supported(g, slices)) return MPSB_ERR_UNSUPPORTED;
+  if (scratch_bytes < ozgemm_scratch_bytes(g, slices)) return MPSB_ERR_INVALID_ARG;
+  MPSB_TRY(get_encoder());
+  const int S = slices;
+  const int64_t Mpad = round_up(g.M, OZ_BM), NBpad = round_up(2 * (int64_t)g.N, OZ_BN);
+  const int64_t Kp = round_up(2 * (int64_t)g.K, OZ_KP_ALIGN);
+  if (Mpad * S >= (int64_t(1) << 31) || NBpad * S >= (int64_t(1) << 31) || Kp >= (int64_t(1) << 31))
+    return MPSB_ERR_UNSUPPORTED;
+  int8_t* sa = static_cast<int8_t*>(scratch);
+  int8_t* sb = sa + (size_t)S * Mpad * Kp;
+  int* ea = reinterpret_cast<int*>(sb + (size_t)S * NBpad * Kp);
+  int* eb = ea + Mpad;
+  MPSB_CUDA_TRY(cudaMemsetAsync(ea, 0, (size_t)(Mpad + NBpad / 2) * sizeof(int), s));
+
+  // A' rows = rows m of op(A): element (m, k) at A[m a_m + k a_k]
+  SliceView va{g.A, g.M, g.K, g.a_m, g.a_k, g.conjA};
+  // B'^T rows come from columns n of op(B): element (n, k) at B[n b_n + k b_k]
+  SliceView vb{g.B, g.N, g.K, g.b_n, g.b_k, g.conjB};
+  const int kc = (int)(Kp / 2);   // complex k extent covered by the slice grid
+  count_launch(ws);
+  oz_rowexp_kernel<<<dim3((unsigned)((g.M + 31) / 32), (unsigned)((g.K + 31) / 32)), 256, 0, s>>>(va, ea);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  count_launch(ws);
+  oz_rowexp_kernel<<<dim3((unsigned)((g.N + 31) / 32), (unsigned)((g.K + 31) / 32)), 256, 0, s>>>(vb, eb);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  count_launch(ws);
+  pick_split(S, false)<<<dim3((unsigned)(Mpad / 32), (unsigned)(kc / 32)), 256, 0, s>>>(va, ea, sa, Mpad, (int)Kp);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  count_launch(ws);
+  pick_split(S, true)<<<dim3((unsigned)(NBpad / 64), (unsigned)(kc / 32)), 256, 0, s>>>(vb, eb, sb, NBpad, (int)Kp);
+  MPSB_CUDA_TRY(cudaGetLastError());
+
+  CUtensorMap ta, tb;
+  MPSB_TRY(make_map(&ta, sa, Kp, S * Mpad, OZ_BM));
+  MPSB_TRY(make_map(&tb, sb, Kp, S * NBpad, OZ_BN));
+  OzParams P;
+  P.M = g.M; P.N = g.N; P.Mpad = (int)Mpad; P.NBpad = (int)NBpad; P.kstages = (int)(Kp / OZ_BK);
+  P.ea = ea; P.eb = eb;
+  P.C = g.C; P.c_m = g.c_m; P.c_n = g.c_n; P.alpha = g.alpha; P.beta = g.beta;
+  P.err = err;
+  OzKernel fn = pick_gemm(S);
+  MPSB_TRY(ensure_kernel_attrs((const void*)fn, smem_of(S)));
+  const int64_t tiles = (Mpad / OZ_BM) * (NBpad / OZ_BN);
+  if (tiles >= (int64_t(1) << 31)) return MPSB_ERR_UNSUPPORTED;
+  count_launch(ws);
+  fn<<<(unsigned)tiles, OZ_THREADS, smem_of(S), s>>>(ta, tb, P);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  return MPSB_OK;
+}
+
+}  // namespace mpsb

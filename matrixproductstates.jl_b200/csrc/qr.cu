@@ -731,15 +731,9 @@ struct Choice {
 
 // Cluster of C = ceil(m / (32 rpl)) CTAs, at most 16: prefer 1 row per lane (measured: the
 // per-CTA work, not the exchange, sets the time), then 2, then 4; the widest panel that fits.
-// MPSB_QR_RPL overrides the rows per lane (tuning).
 bool choose(int m, int n, Choice& ch) {
-  static const int env_rpl = [] {
-    const char* s = getenv("MPSB_QR_RPL");
-    return s ? atoi(s) : 0;
-  }();
   QrParams P;
   for (int rpl : {1, 2, 4}) {
-    if (env_rpl > 0 && rpl != env_rpl) continue;
     const int rows = 32 * rpl;
     const int C = (m + rows - 1) / rows;
     if (C > CMAX) continue;
@@ -789,13 +783,7 @@ int launch_factor(const QrProblem& p, const Choice& ch, cd* Vb, cd* Tb, cudaStre
   P.Tg = Tb;
   QrKernel fn = kernel_for(ch.rpl, ch.nb);
   if (!fn) return MPSB_ERR_UNSUPPORTED;
-  static bool attr_done[3][8] = {};
-  bool& done = attr_done[ch.nb == 16 ? 2 : (ch.nb == 8 ? 1 : 0)][ch.rpl];
-  if (!done) {
-    MPSB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT));
-    MPSB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    done = true;
-  }
+  MPSB_TRY(ensure_kernel_attrs((const void*)fn, (int)SMEM_LIMIT, true));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(ch.C, p.batch, 1);
   cfg.blockDim = dim3(NT, 1, 1);
@@ -830,7 +818,7 @@ int form_q(const QrProblem& p, int nb, const cd* Vb, const cd* Tb, cd* Gb, cd* M
   }
   {  // M = T V1^H
     const size_t smem = tmat_smem(n, nb) <= SMEM_LIMIT ? tmat_smem(n, nb) : 0;
-    if (smem) MPSB_CUDA_TRY(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT));
+    if (smem) MPSB_TRY(ensure_kernel_attrs((const void*)tk, (int)SMEM_LIMIT));
     count_launch(ws);
     tk<<<dim3((n + TR_WARPS - 1) / TR_WARPS, p.batch), 32 * TR_WARPS, smem, s>>>(m, n, nb, Vb, Tb, Gb, Mb);
     MPSB_CUDA_TRY(cudaGetLastError());

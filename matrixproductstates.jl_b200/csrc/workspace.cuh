@@ -14,6 +14,7 @@ struct Workspace {
   DevBuf splitk;          // split-K partial tiles
   DevBuf qr;              // QR: reflectors, tau, V^H V and T V1^H
   DevBuf svd;             // SVD: the Jacobi working matrix, V, norms, flags
+  DevBuf oz;              // sliced tensor-core GEMM: int8 slices of both operands, row exponents
   DevBuf named[16];       // per-sweep temporaries (see engine.cu)
   bool capturing = false;
   int64_t launches = 0;   // kernel launches issued (eager) or recorded (capture)
@@ -40,6 +41,21 @@ inline int devbuf_ensure(Workspace* ws, DevBuf& b, size_t bytes) {
   }
   b.cap = want;
   return MPSB_OK;
+}
+
+// every device buffer of a workspace (context teardown)
+inline void ws_free(Workspace& w) {
+  DevBuf* all[] = {&w.splitk, &w.qr, &w.svd, &w.oz};
+  for (DevBuf* b : all) {
+    if (b->p) cudaFree(b->p);
+    b->p = nullptr;
+    b->cap = 0;
+  }
+  for (DevBuf& b : w.named) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+  }
 }
 
 inline int ws_splitk(Workspace* ws, size_t bytes, cd** out) {

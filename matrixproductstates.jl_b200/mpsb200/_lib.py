@@ -36,6 +36,7 @@ SIGNATURES = {
     "mpsb_ctx_set_stream": ([_vp, _vp], _i),
     "mpsb_ctx_set_graphs": ([_vp, _i], _i),
     "mpsb_ctx_set_pipeline": ([_vp, _i], _i),
+    "mpsb_ctx_set_precision": ([_vp, _i, _i], _i),
     "mpsb_ctx_launch_count": ([_vp, _pi64], _i),
     "mpsb_mps_create": ([_vp, _i, _i, _pi64, _pvp], _i),
     "mpsb_mps_destroy": ([_vp], _i),
@@ -81,6 +82,7 @@ SIGNATURES = {
     "mpsb_compress_sum_var_apply_H_two_site": ([_vp, _vp, _pd, _i, _pvp, _vp, _i, _d, _i, _i, _pvp], _i),
     "mpsb_op_svd": ([_vp, _vp, _vp, _pd, _vp, _i, _i], _i),
     "mpsb_op_qr": ([_vp] * 4 + [_i] * 2, _i),
+    "mpsb_op_zgemm": ([_vp, _i, _i, _i, _vp, _i64, _i64, _i, _vp, _i64, _i64, _i, _vp, _i64, _i64, _pd, _pd, _i], _i),
     "mpsb_op_prod_AOR_noalloc": ([_vp] * 5 + [_i] * 6, _i),
 }
 

@@ -50,6 +50,11 @@ class Context:
         on a second stream (default on; identical results)."""
         _lib.call("mpsb_ctx_set_pipeline", self.h, 1 if enable else 0)
 
+    def set_precision(self, slices, min_tiles=64):
+        """Contraction precision of the sweeps: 0 = FP64; 3..7 = int8-sliced tensor-core GEMMs
+        with that many slices per operand for GEMMs of at least ``min_tiles`` output tiles."""
+        _lib.call("mpsb_ctx_set_precision", self.h, int(slices), int(min_tiles))
+
     def set_stream(self, stream_ptr):
         _lib.call("mpsb_ctx_set_stream", self.h, C.c_void_p(stream_ptr or 0))
 
