@@ -453,7 +453,129 @@ def run_ours(args, rank, world, local_rank, dist):
     return line
 
 
+def _event_us(torch, stream, fn, reps, warmup, ctx):
+    for _ in range(warmup):
+        fn()
+    ctx.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    return e0.elapsed_time(e1) * 1e3 / reps
+
+
+def run_op(argv):
+    """Per-operation timing through the C ABI (CUDA events, one GPU), one JSON line; small
+    enough to run under a profiler with --reps 1:
+
+        bench.py --op qr M N                     mpsb_op_qr (leftorth!/rightorth!, src/orthonormalisation.jl:164-234)
+        bench.py --op gemm-mix [--chi --d --w]   prod_LR (3,4) / (4,3), update_re!, update_le! of one interior site
+        bench.py --op zgemm M N K [--slices S]   mpsb_op_zgemm, FP64 (S=0) or int8-sliced tensor-core path
+        bench.py --op rk4 [N] [--chi --w --slices S --random CHI0]
+                                                 in-place RK4 steps of the density-matrix workload, each timed
+                                                 step inside an NVTX range "rk4_step"
+    """
+    ap = argparse.ArgumentParser(prog="bench.py --op")
+    ap.add_argument("op", choices=["qr", "gemm-mix", "zgemm", "rk4"])
+    ap.add_argument("dims", nargs="*", type=int)
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--chi", type=int, default=128)
+    ap.add_argument("--d", type=int, default=4)
+    ap.add_argument("--w", type=int, default=8)
+    ap.add_argument("--slices", type=int, default=0)
+    ap.add_argument("--random", type=int, default=0, help="rk4: start from a random MPS of this bond dim")
+    a = ap.parse_args(argv)
+
+    import ctypes as C
+
+    import torch
+
+    import __graft_entry__
+    __graft_entry__.build()
+    import mpsb200 as K
+    from mpsb200 import _lib
+
+    ctx = K.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    out = {"op": a.op}
+    if a.op == "qr":
+        m, n = a.dims[:2] if len(a.dims) >= 2 else (512, 128)
+        X = torch.randn(m * n, dtype=torch.complex128, device="cuda", generator=g)
+        Q = torch.empty_like(X)
+        torch.cuda.synchronize()
+        args = (C.c_void_p(X.data_ptr()), C.c_void_p(Q.data_ptr()), None, m, n)
+        us = _event_us(torch, stream, lambda: _lib.call("mpsb_op_qr", ctx.h, *args), a.reps, a.warmup, ctx)
+        flops = 16.0 * (m * n * n - n ** 3 / 3.0)   # factorisation + forming Q (complex)
+        out.update({"m": m, "n": n, "us": us, "tflops": flops / us / 1e6})
+    elif a.op == "zgemm":
+        M, N, Kd = a.dims[:3] if len(a.dims) >= 3 else (512, 2048, 4096)
+        A = torch.randn(M * Kd, dtype=torch.complex128, device="cuda", generator=g)
+        B = torch.randn(Kd * N, dtype=torch.complex128, device="cuda", generator=g)
+        Cm = torch.zeros(M * N, dtype=torch.complex128, device="cuda")
+        torch.cuda.synchronize()
+        args = (ctx.h, M, N, Kd, C.c_void_p(A.data_ptr()), 1, M, 1, C.c_void_p(B.data_ptr()), 1, Kd, 0,
+                C.c_void_p(Cm.data_ptr()), 1, M, None, None, a.slices)
+        us = _event_us(torch, stream, lambda: _lib.call("mpsb_op_zgemm", *args), a.reps, a.warmup, ctx)
+        out.update({"M": M, "N": N, "K": Kd, "slices": a.slices, "us": us, "tflops": 8.0 * M * N * Kd / us / 1e6})
+    elif a.op == "rk4":
+        from mpsb200 import drivers as GDR, models as GM
+        na = a.dims[0] if a.dims else 40
+        ctx.set_precision(a.slices)
+        p = GM.WaveguideChain(na, gam_eg=0.1, omega=0.5, gam_phi=0.1)
+        rho = None
+        if a.random:
+            import numpy as np
+            rho, _ = K.mpsrandom(na, a.random, 4, np.random.default_rng(60), ctx)
+            K.normalize_lo_(rho)
+            rho, _ = K.expandmps(rho, a.chi, ctx)
+        b = GDR.DensityBuffers(p, a.chi, 0.005, a.w, ctx, rho)
+        for _ in range(a.warmup):
+            b.step()
+        ctx.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.reps):
+            torch.cuda.nvtx.range_push("rk4_step")
+            b.step()
+            torch.cuda.nvtx.range_pop()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ctx.sync()
+        ms = e0.elapsed_time(e1) / a.reps
+        out.update({"na": na, "chi": a.chi, "w": a.w, "slices": a.slices, "random_start": a.random,
+                    "ms_per_step": ms, "site_updates_per_s": na / ms * 1e3})
+    else:
+        chi, d, w = a.chi, a.d, a.w
+        bufs = [torch.randn(chi * w * d * chi, dtype=torch.complex128, device="cuda", generator=g) for _ in range(3)]
+        torch.cuda.synchronize()
+        p = [C.c_void_p(b.data_ptr()) for b in bufs]
+        calls = [
+            ("prod_LR_3_4", "mpsb_op_prod_LR_3_4", (p[0], p[1], p[2], chi, w, chi, d, chi)),
+            ("update_re", "mpsb_op_update_re", (p[2], p[1], p[0], chi, w, d, chi, chi)),
+            ("prod_LR_4_3", "mpsb_op_prod_LR_4_3", (p[0], p[1], p[2], chi, d, chi, w, chi)),
+            ("update_le", "mpsb_op_update_le", (p[2], p[0], p[1], chi, d, chi, w, chi)),
+        ]
+        flops = 8.0 * w * d * chi ** 3
+        tot = 0.0
+        for tag, name, args in calls:
+            us = _event_us(torch, stream, lambda: _lib.call(name, ctx.h, *args), a.reps, a.warmup, ctx)
+            out[tag] = {"us": us, "tflops": flops / us / 1e6}
+            tot += us
+        out.update({"chi": chi, "d": d, "w": w, "mix_us": tot, "mix_tflops": 4 * flops / tot / 1e6})
+    ctx.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
+    if "--op" in sys.argv:
+        i = sys.argv.index("--op")
+        return run_op(sys.argv[i + 1:])
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)

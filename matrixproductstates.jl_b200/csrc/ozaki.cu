@@ -109,13 +109,21 @@ __device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
 __host__ __device__ constexpr uint32_t idesc_i8() {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
 }
+// A-operand collector use across consecutive MMAs that share A: 0 = read A (no reuse),
+// 1 = read and keep it, 2 = reuse the kept A, 3 = reuse it for the last time
+#define MPSB_MMA_I8(QUAL)                                                                          \
+  asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"                                        \
+               "tcgen05.mma.cta_group::1.kind::i8" QUAL " [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d), \
+               "l"(adesc), "l"(bdesc), "r"(idesc_i8()), "r"(accumulate)                             \
+               : "memory")
+template <int COLLECT>
 __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc_i8()), "r"(accumulate)
-      : "memory");
+  if (COLLECT == 1) MPSB_MMA_I8(".collector::a::fill");
+  else if (COLLECT == 2) MPSB_MMA_I8(".collector::a::use");
+  else if (COLLECT == 3) MPSB_MMA_I8(".collector::a::lastuse");
+  else MPSB_MMA_I8("");
 }
+#undef MPSB_MMA_I8
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
                : "memory");
@@ -338,7 +346,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             for (int j = 0; j < S - i; ++j) {
               const uint64_t bd = smem_desc_sw64(st + S * A_TILE + j * B_TILE + kk * 32);
               const uint32_t acc = (kb > 0 || kk > 0 || i > 0) ? 1u : 0u;   // i == 0 opens every level
-              mma_i8(tmem + (uint32_t)((i + j) * OZ_BN), ad, bd, acc);
+              const uint32_t td = tmem + (uint32_t)((i + j) * OZ_BN);
+              // A_i is shared by the S - i products of this row of the slice triangle
+              if (S - i == 1) mma_i8<0>(td, ad, bd, acc);
+              else if (j == 0) mma_i8<1>(td, ad, bd, acc);
+              else if (j == S - i - 1) mma_i8<3>(td, ad, bd, acc);
+              else mma_i8<2>(td, ad, bd, acc);
             }
           }
         }
