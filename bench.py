@@ -1,17 +1,25 @@
 #!/usr/bin/env python
 """Benchmark of the RK4 MPS/MPO time step (RK4stp_apply_H_half!, src/timeevolution.jl:178-196).
 
-Workload (default): vectorised density matrix of the driven waveguide spin chain, N=40 sites,
-d=4, bond dim chi=128, Lindbladian MPO of width w=8 (the exact w=6 MPO plus two zero channels),
-dt=0.005, started from the all-down product state; one step = one in-place 4-stage RK4 step
-(10-argument form) of the whole chain.  Metric: site-updates/s = sites x steps / time.
+Workload (default, --workload precision): vectorised density matrix of the driven waveguide spin
+chain, N=60 sites, d=4, bond dim chi=512, Lindbladian MPO of width w=8 (the exact w=6 MPO plus
+two zero channels), dt=0.005, started from a random chi=64 MPS (complex Gaussian, seed 60,
+left-orthogonal, unit norm) zero-padded to chi=512; one step = one in-place 4-stage RK4 step
+(10-argument form) of the whole chain.  Metric: site-updates/s = sites x steps / time, with the
+step's contractions on the int8-sliced tensor-core path (6 slices) and its QR / norms in FP64;
+the plain FP64 path is timed on the same state beside it, and the observables of the two are
+compared after every warm-up step (the error of the split path against FP64) and against the
+oracle's golden values of the first steps.  --workload density: the plain-FP64 configuration
+(N=40, chi=128, all-down start).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload precision|density]
+    python bench.py --op qr|gemm-mix|zgemm|rk4 ...        per-operation timing (see run_op)
 
 Our arm: device-resident state, CUDA-event timing of K steps on the library stream (max over
 ranks); each rank evolves its own independent density matrix (replicas, weak scaling).
 Reference arm (--impl reference): the CPU oracle (NumPy/OpenBLAS restatement of the
-reference's Julia code, which cannot run here) on the host cores, rank 0 only.
+reference's Julia code, which cannot run here) on the host cores, rank 0 only, on a bounded
+sample of the workload.
 """
 import argparse
 import json
@@ -19,7 +27,6 @@ import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -28,14 +35,17 @@ for _p in (ROOT, PKG):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
-WORKLOAD = dict(na=40, d=4, chi=128, w=8, dt=0.005, gam_eg=0.1, omega=0.5, gam_phi=0.1)
-METRIC = "MPS site-updates/s (RK4 step, complex128)"
+WORKLOADS = {
+    "precision": dict(na=60, d=4, chi=512, chi0=64, seed=60, w=8, dt=0.005, gam_eg=0.1, omega=0.5, gam_phi=0.1,
+                      slices=6, pairs=((0, 1), (29, 30), (9, 49)), golden="rho_n60_chi512.npz"),
+    "density": dict(na=40, d=4, chi=128, chi0=0, seed=0, w=8, dt=0.005, gam_eg=0.1, omega=0.5, gam_phi=0.1,
+                    slices=0, pairs=((0, 1), (9, 10), (19, 20), (4, 34)), golden="rho_n40_chi128.npz"),
+}
+METRIC = "MPS site-updates/s (RK4 step)"
 UNIT = "site-updates/s"
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch, from one ncu capture each:
-# qr_kernel at the workload's interior-site QR shape (512 x 128; the input read once, the
-# outputs stay in L2) and zgemm_kernel at the 3-index prod_LR shape (M=128, N=512, K=1024)
+# dram__bytes_read.sum + dram__bytes_write.sum of one cluster-QR launch at the chi=128 interior
+# shape (512 x 128; the input read once, the outputs stay in L2), from one ncu capture
 QR_TRAFFIC_BYTES = 1114624
-GEMM_TRAFFIC_BYTES = 10551296
 
 
 def dims_rule(na, dmax, d):
@@ -159,27 +169,6 @@ def cpu_info():
     return model, os.cpu_count()
 
 
-def oracle_step_rate(nsteps):
-    """The CPU oracle (NumPy + OpenBLAS, all host threads) on the same workload."""
-    from oracle import models as OM
-    from oracle import mps_ref as R
-    W = WORKLOAD
-    na, chi, w, dt = W["na"], W["chi"], W["w"], W["dt"]
-    p = OM.SpinChain(na, gam_eg=W["gam_eg"], omega=W["omega"], gam_phi=W["gam_phi"])
-    rho, dims = R.mpsgroundstate(na, chi, W["d"])
-    r1, r2, r3 = (R.copy_mps(rho) for _ in range(3))
-    env = [R.build_env(dims, dims) for _ in range(3)]
-    envop = R.build_env(dims, dims, [w] * (na + 1))
-    L = [OM.construct_L_spin_model(p, 1, dt / 2, 0, w), OM.construct_L_spin_model(p, 0, 1, dt / 2, w),
-         OM.construct_L_spin_model(p, 1, dt / 2, dt, w)]
-    times = []
-    for _ in range(nsteps):
-        t0 = time.perf_counter()
-        R.RK4stp_apply_H_half_(dt, L, rho, rho, r1, r2, r3, *env, envop)
-        times.append(time.perf_counter() - t0)
-    return times
-
-
 def max_over_ranks(x, dist, device="cuda"):
     """The largest of the ranks' x, on every rank (x itself without a process group): the
     job's time is its slowest replica's."""
@@ -196,117 +185,6 @@ def job_rate(world, sites, steps, secs):
     return world * sites * steps / secs
 
 
-def run_reference(args, rank):
-    if rank != 0:
-        return None
-    model, cores = cpu_info()
-    W = WORKLOAD
-    for _ in range(args.warmup):
-        oracle_step_rate(1)
-    times = oracle_step_rate(args.steps)
-    tot = sum(times)
-    value = W["na"] * args.steps / tot
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
-        "data": "synthetic (all-down product rho, waveguide Lindbladian)",
-        "config": config_dict(args),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": "%d full RK4 steps of the workload on the CPU oracle (NumPy/OpenBLAS %s, %d threads)"
-                                   % (args.steps, model, cores)},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    return line
-
-
-def config_dict(args):
-    W = WORKLOAD
-    return {"workload": "density-matrix RK4 step, waveguide spin chain N=%d, d=%d, chi=%d, w=%d (6 + 2 zero "
-                        "channels), dt=%g" % (W["na"], W["d"], W["chi"], W["w"], W["dt"]),
-            "sites": W["na"], "d": W["d"], "chi": W["chi"], "w": W["w"], "dt": W["dt"],
-            "parallelism": "replicas x%d (independent rho per GPU)" % args.gpus,
-            "l2": "working set per step ~230 MB > 126 MB L2 (no flush needed)"}
-
-
-def measure_fp64_peak(torch):
-    """cuBLAS zgemm throughput (the FP64 denominator; the peaks file has HBM and bf16 only)."""
-    n = 4096
-    a = torch.randn(n, n, dtype=torch.complex128, device="cuda")
-    b = torch.randn(n, n, dtype=torch.complex128, device="cuda")
-    for _ in range(2):
-        torch.matmul(a, b)
-    torch.cuda.synchronize()
-    best = 1e30
-    for _ in range(5):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        torch.matmul(a, b)
-        e1.record()
-        torch.cuda.synchronize()
-        best = min(best, e0.elapsed_time(e1) / 1e3)
-    del a, b
-    return 8.0 * n ** 3 / best / 1e12
-
-
-def time_gemm_mix(K, ctx, torch, stream):
-    """CUDA-event timing of the zgemm kernel on the four GEMM shapes of an interior site
-    (prod_LR!/update_re!/update_le! at chi=128, d=4, w=8): returns (flops, seconds) per mix."""
-    import ctypes as C
-    from mpsb200 import _lib
-    W = WORKLOAD
-    chi, d, w = W["chi"], W["d"], W["w"]
-    bufs = [torch.randn(chi * w * d * chi, dtype=torch.complex128, device="cuda") for _ in range(3)]
-    torch.cuda.synchronize()
-    p = [C.c_void_p(b.data_ptr()) for b in bufs]
-    calls = [
-        ("mpsb_op_prod_LR_3_4", (p[0], p[1], p[2], chi, w, chi, d, chi), 8.0 * chi * (d * chi) * (chi * w)),
-        ("mpsb_op_update_re", (p[2], p[1], p[0], chi, w, d, chi, chi), 8.0 * (chi * w) * chi * (d * chi)),
-        ("mpsb_op_prod_LR_4_3", (p[0], p[1], p[2], chi, d, chi, w, chi), 8.0 * (chi * d) * chi * (chi * w)),
-        ("mpsb_op_update_le", (p[2], p[0], p[1], chi, d, chi, w, chi), 8.0 * (chi * w) * chi * (chi * d)),
-    ]
-    reps = 20
-    for name, a, _ in calls:
-        _lib.call(name, ctx.h, *a)
-    ctx.sync()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        for name, a, _ in calls:
-            _lib.call(name, ctx.h, *a)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    secs = e0.elapsed_time(e1) / 1e3 / reps
-    flops = sum(c[2] for c in calls)
-    return flops, secs, len(calls)
-
-
-def time_qr(ctx, torch, stream):
-    """CUDA-event timing of one QR of the interior-site shape (d*chi x chi) through the op API:
-    returns (algorithmic flops, seconds) per QR."""
-    import ctypes as C
-    from mpsb200 import _lib
-    W = WORKLOAD
-    m, n = W["d"] * W["chi"], W["chi"]
-    g = torch.Generator(device="cuda").manual_seed(7)
-    X = torch.randn(m * n, dtype=torch.complex128, device="cuda", generator=g)
-    Q = torch.empty_like(X)
-    torch.cuda.synchronize()
-    args = (C.c_void_p(X.data_ptr()), C.c_void_p(Q.data_ptr()), None, m, n)
-    for _ in range(3):
-        _lib.call("mpsb_op_qr", ctx.h, *args)
-    ctx.sync()
-    reps = 10
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        _lib.call("mpsb_op_qr", ctx.h, *args)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ctx.sync()
-    return 16.0 * (m * n * n - n ** 3 / 3.0), e0.elapsed_time(e1) / 1e3 / reps, m, n
-
-
 def run_serving():
     """p50/p99 job latency of a bounded sample of the mixed serving stream: 24 seeded Poisson
     arrivals at 200 jobs/s, 70% trajectories (N 20..40, chi 16/32/64, d=2, w=4) and 30%
@@ -320,137 +198,6 @@ def run_serving():
             "queue_p50_ms": 1e3 * st["queue_p50_s"], "site_updates_per_s": st["site_updates_per_s"],
             "wall_s": st["wall_s"],
             "sample": "24 jobs: 70% trajectories N 20..40 chi<=64, 30% rho N 8..16 chi<=32, 10..30 steps"}
-
-
-def run_ours(args, rank, world, local_rank, dist):
-    import numpy as np
-    import torch
-
-    import mpsb200 as K
-    from mpsb200 import drivers as GDR
-    from mpsb200 import models as GM
-
-    torch.cuda.set_device(local_rank)
-    W = WORKLOAD
-    ctx = K.Context(local_rank)
-    stream = torch.cuda.Stream()
-    ctx.set_stream(stream.cuda_stream)
-    p = GM.WaveguideChain(W["na"], gam_eg=W["gam_eg"], omega=W["omega"], gam_phi=W["gam_phi"])
-    b = GDR.DensityBuffers(p, W["chi"], W["dt"], W["w"], ctx)
-    dims = b.dims
-    wv = [1] + [W["w"]] * (W["na"] - 1) + [1]
-    fl = step_flops(dims, wv, W["d"])
-    for _ in range(args.warmup):
-        b.step()
-    ctx.sync()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local_rank)
-    sampler.start()
-    l0 = ctx.launches
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        # one NVTX range per timed step, so a profiler can keep exactly these launches
-        # (ncu --nvtx --nvtx-include "rk4_step/")
-        torch.cuda.nvtx.range_push("rk4_step")
-        b.step()
-        torch.cuda.nvtx.range_pop()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    launches = ctx.launches - l0
-    secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
-    value = job_rate(world, W["na"], args.steps, secs)
-    tr, see, _ = b.observables(pairs=())
-
-    # ---- end to end through the public API with host buffers: every step uploads the three
-    # generator MPOs from pinned host memory (the reference loop's update_L!/update_h! refresh)
-    # and reads Tr(rho) back (the measurement of the example loop)
-    mpo_host = []
-    h2d = 0
-    for t_, (con, delt, tt) in enumerate([(1, W["dt"] / 2, 0.0), (0, 1, W["dt"] / 2), (1, W["dt"] / 2, W["dt"])]):
-        sites = GM.construct_L_spin_model(p, con, delt, tt, W["w"])
-        pinned = []
-        for s in sites:
-            pt = torch.empty(s.size * 2, dtype=torch.float64, pin_memory=True)
-            arr = pt.numpy()
-            arr[:] = np.ascontiguousarray(s.ravel(order="F")).view(np.float64)
-            pinned.append((pt, arr.reshape(-1)))
-            h2d += s.size * 16
-        mpo_host.append(pinned)
-    ke = max(2, args.steps)
-    import ctypes as C
-    from mpsb200 import _lib
-
-    def e2e_step():
-        for mpo, pinned in zip(b.L, mpo_host):
-            for k, (_, arr) in enumerate(pinned):
-                _lib.call("mpsb_mpo_set_site", mpo.h, k + 1, arr.ctypes.data_as(C.POINTER(C.c_double)))
-        b.step()
-        K.scal_prod_no_conj(b.trace_fn, b.rho)
-
-    for _ in range(args.warmup):   # the first host-buffer steps carry one-time costs
-        e2e_step()
-    ctx.sync()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(ke):
-        e2e_step()
-    ctx.sync()
-    e2e_secs = max_over_ranks(time.perf_counter() - t0, dist)
-    e2e_value = job_rate(world, W["na"], ke, e2e_secs)
-
-    # ---- roofline of the dominant kernel (the cluster QR, ~43% of the step by the ncu launch
-    # list) at the workload's interior-site shape, and of the zgemm kernel on the site's GEMMs
-    peak = measure_fp64_peak(torch)
-    qflops, qsecs, qm, qn = time_qr(ctx, torch, stream)
-    qach = qflops / qsecs / 1e12
-    roofline = {"bound": "tensor", "pipe": "fp64", "limiter": "latency (128 sequential column steps)",
-                "kernel": "qr_kernel (cluster Householder factorisation) + Q formation (2 zgemm_kernel, qr_tmat_kernel)",
-                "achieved": qach, "peak": peak, "unit": "TFLOP/s", "frac": qach / peak,
-                "peak_source": "cuBLAS zgemm 4096^3 measured in this run (no FP64 entry in MEASURED_PEAKS.json)",
-                "traffic": QR_TRAFFIC_BYTES,
-                "per_launch": "one QR of %d x %d (d*chi x chi): 16(mn^2 - n^3/3) = %.3e flops in %.1f us; "
-                              "traffic = qr_kernel dram read+write (ncu)" % (qm, qn, qflops, qsecs * 1e6)}
-    gflops, gsecs, ncalls = time_gemm_mix(K, ctx, torch, stream)
-    gach = gflops / gsecs / 1e12
-    roofline_gemm = {"bound": "tensor", "pipe": "fp64", "kernel": "zgemm_kernel",
-                     "achieved": gach, "peak": peak, "unit": "TFLOP/s", "frac": gach / peak,
-                     "traffic": GEMM_TRAFFIC_BYTES,
-                     "per_launch": "flop-weighted mean over the %d GEMM shapes of an interior site "
-                                   "(chi=128, d=4, w=8): %.3e flops in %.1f us; traffic = the prod_LR launch "
-                                   "(M=128, N=512, K=1024) dram read+write (ncu)" % (ncalls, gflops, gsecs * 1e6)}
-    serving = None
-    if world == 1 and not args.no_serve:
-        serving = run_serving()
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
-        "data": "synthetic (all-down product rho, waveguide Lindbladian)",
-        "config": config_dict(args),
-        "clocks": clocks,
-        "gpu_launches": int(launches),
-        "step_tflops": sum(fl.values()) * args.steps / secs * world / 1e12,
-        "step_flops": fl,
-        "roofline": roofline,
-        "roofline_gemm": roofline_gemm,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16,
-                "steps": ke},
-        "check": {"trace_rho": tr.real, "max_see": float(np.max(see.real))},
-        "serving": serving,
-    }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        model, cores = cpu_info()
-        times = oracle_step_rate(1)
-        line["cpu_baseline"] = {"value": W["na"] / times[0], "unit": UNIT, "cores": cores, "kind": "port",
-                                "sample": "1 full RK4 step of the workload on the CPU oracle (NumPy/OpenBLAS, "
-                                          "%s, %d threads): %.2f s" % (model, cores, times[0])}
-    ctx.close()
-    return line
 
 
 def _event_us(torch, stream, fn, reps, warmup, ctx):
@@ -572,15 +319,404 @@ def run_op(argv):
     print(json.dumps(out), flush=True)
 
 
+def load_peaks():
+    """(int8 dense TOP/s, source) for the sliced GEMM's roofline: twice the measured dense bf16
+    rate of MEASURED_PEAKS.json (the int8 kind runs the same tensor pipe at twice the bf16
+    rate), else twice the pool's fallback bf16 figure."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        bf16 = float(pk.get("bf16_tflops"))
+        return 2.0 * bf16, "2 x bf16_tflops %.1f of measured (MEASURED_PEAKS.json)" % bf16
+    except Exception:
+        return 2.0 * 1590.0, "2 x 1590 TFLOP/s bf16 of fallback (no MEASURED_PEAKS.json)"
+
+
+def workload_buffers(W, ctx, slices):
+    """Device buffers of the workload's density matrix on ctx, contractions at `slices`."""
+    import numpy as np
+
+    import mpsb200 as K
+    from mpsb200 import drivers as GDR
+    from mpsb200 import models as GM
+    ctx.set_precision(slices)
+    p = GM.WaveguideChain(W["na"], gam_eg=W["gam_eg"], omega=W["omega"], gam_phi=W["gam_phi"])
+    rho = None
+    if W["chi0"]:
+        rho, _ = K.mpsrandom(W["na"], W["chi0"], W["d"], np.random.default_rng(W["seed"]), ctx)
+        K.normalize_lo_(rho)
+        rho, _ = K.expandmps(rho, W["chi"], ctx)
+    return GDR.DensityBuffers(p, W["chi"], W["dt"], W["w"], ctx, rho), p
+
+
+def obs_error(a, b):
+    """max |difference| of two (Tr rho, <see_i>, <s+_i s-_j>) records and the records' scale"""
+    import numpy as np
+    err = max(abs(a[0] - b[0]), float(np.abs(np.asarray(a[1]) - np.asarray(b[1])).max()),
+              float(np.abs(np.asarray(a[2]) - np.asarray(b[2])).max()))
+    scale = max(abs(b[0]), float(np.abs(np.asarray(b[1])).max()), float(np.abs(np.asarray(b[2])).max()))
+    return err, scale
+
+
+def oracle_site_sample(W, threads_note=""):
+    """One interior site-update on the CPU oracle: every contraction and QR that an interior site
+    (chi x d x chi, MPO bonds w) undergoes in the four stages of one RK4 step, in the sweeps'
+    order (environment initialisation, plain terms, the operator term, the QR, environment
+    updates), on seeded random tensors.  Returns (seconds, algorithmic flops of the sample)."""
+    import numpy as np
+
+    from oracle import mps_ref as R
+    chi, d, w = W["chi"], W["d"], W["w"]
+    rng = np.random.default_rng(1)
+
+    def cr(*s):
+        return (rng.standard_normal(s) + 1j * rng.standard_normal(s)).astype(np.complex128)
+    A, A0 = cr(chi, d, chi), cr(chi, d, chi)
+    O = cr(w, d, w, d)
+    F3L, F3R = cr(chi, w, chi), cr(chi, w, chi)
+    F2 = cr(chi, chi)
+    flops = [0.0]
+
+    def g(m, n, k):
+        flops[0] += 8.0 * m * n * k
+    t0 = time.perf_counter()
+    for right, npl in ((False, 0), (True, 1), (False, 1), (True, 3)):
+        for _ in range(npl):                      # environment initialisation, plain terms
+            if right:
+                AR = R.prod_LR(A, F2); g(chi * d, chi, chi)
+                R.update_renv(A0, AR); g(chi, chi, d * chi)
+            else:
+                AL = R.prod_LR(F2, A); g(chi, d * chi, chi)
+                R.update_lenv(A0, AL); g(chi, chi, chi * d)
+        if right:                                 # environment initialisation, operator term
+            T = R.prod_AOR(A, O, F3R); g(chi * d, w * chi, chi); flops[0] += 8.0 * chi * chi * d * w * w * d
+            R.update_re(A0, T); g(chi * w, chi, d * chi)
+        else:
+            T = R.prod_AOL(A, O, F3L); g(w * chi, d * chi, chi); flops[0] += 8.0 * chi * chi * d * w * w * d
+            R.update_le(A0, T); g(chi * w, chi, chi * d)
+        for _ in range(npl):                      # the sweep: plain terms
+            P = R.prod_LR(F2, A); g(chi, d * chi, chi)
+            R.prod_LR(P, F2); g(chi * d, chi, chi)
+        if right:                                 # operator term, QR, environment updates
+            T = R.prod_AOL(A, O, F3L); g(w * chi, d * chi, chi); flops[0] += 8.0 * chi * chi * d * w * w * d
+            B = R.prod_LR(T, F3R); g(chi * d, chi, chi * w)
+            Q = R.leftorth_(B); flops[0] += 16.0 * (d * chi * chi * chi - chi ** 3 / 3.0)
+            for _ in range(npl):
+                R.update_lenv(Q, P); g(chi, chi, chi * d)
+            R.update_le(Q, T); g(chi * w, chi, chi * d)
+        else:
+            T = R.prod_AOR(A, O, F3R); g(chi * d, w * chi, chi); flops[0] += 8.0 * chi * chi * d * w * w * d
+            B = R.prod_LR(F3L, T); g(chi, d * chi, chi * w)
+            Q = R.rightorth_(B); flops[0] += 16.0 * (d * chi * chi * chi - chi ** 3 / 3.0)
+            for _ in range(npl):
+                R.update_renv(Q, P); g(chi, chi, d * chi)
+            R.update_re(Q, T); g(chi * w, chi, d * chi)
+    return time.perf_counter() - t0, flops[0]
+
+
+def cpu_rate(W, nsamples):
+    """Chain-average site-updates/s of the CPU oracle: interior site-update samples scaled by
+    the flop model's ratio of the interior site to the chain's mean site."""
+    dims = dims_rule(W["na"], W["chi"], W["d"])
+    wv = [1] + [W["w"]] * (W["na"] - 1) + [1]
+    mean_site = sum(step_flops(dims, wv, W["d"]).values()) / W["na"]
+    times, fl = [], 0.0
+    for _ in range(nsamples):
+        t, fl = oracle_site_sample(W)
+        times.append(t)
+    tot = sum(times)
+    return nsamples * (fl / mean_site) / tot, tot / nsamples, fl, mean_site
+
+
+def config_dict(args, W):
+    return {"workload": "density-matrix RK4 step, waveguide spin chain N=%d, d=%d, chi=%d, w=%d (6 + 2 zero "
+                        "channels), dt=%g, %s start%s" % (
+                            W["na"], W["d"], W["chi"], W["w"], W["dt"],
+                            ("random chi=%d (seed %d) zero-padded" % (W["chi0"], W["seed"])) if W["chi0"]
+                            else "all-down product",
+                            (", contractions int8-sliced x%d on tcgen05, QR/norms FP64" % W["slices"])
+                            if W["slices"] else ", FP64"),
+            "name": args.workload, "sites": W["na"], "d": W["d"], "chi": W["chi"], "w": W["w"], "dt": W["dt"],
+            "slices": W["slices"],
+            "parallelism": "replicas x%d (independent rho per GPU)" % args.gpus,
+            "l2": "working set per step > 126 MB L2 (no flush needed)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    W = WORKLOADS[args.workload]
+    model, cores = cpu_info()
+    for _ in range(args.warmup):
+        oracle_site_sample(W)
+    value, t_sample, fl, mean_site = cpu_rate(W, args.steps)
+    sample = ("%d interior site-updates (chi=%d, d=%d, w=%d: all contractions and the QR of one site in the "
+              "four stages of an RK4 step) on the CPU oracle (NumPy/OpenBLAS, %s, %d threads), %.2f s each; "
+              "chain-average rate = interior rate x interior/mean site flops (%.3g/%.3g)"
+              % (args.steps, W["chi"], W["d"], W["w"], model, cores, t_sample, fl, mean_site))
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * W["na"] / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+        "data": "synthetic (seeded random tensors of the workload's interior shapes)",
+        "config": config_dict(args, W),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def time_qr(ctx, torch, stream, m, n):
+    """CUDA-event timing of one QR of the interior-site shape (d*chi x chi) through the op API:
+    returns (algorithmic flops, seconds) per QR."""
+    import ctypes as C
+    from mpsb200 import _lib
+    g = torch.Generator(device="cuda").manual_seed(7)
+    X = torch.randn(m * n, dtype=torch.complex128, device="cuda", generator=g)
+    Q = torch.empty_like(X)
+    torch.cuda.synchronize()
+    args = (C.c_void_p(X.data_ptr()), C.c_void_p(Q.data_ptr()), None, m, n)
+    us = _event_us(torch, stream, lambda: _lib.call("mpsb_op_qr", ctx.h, *args), 5, 2, ctx)
+    del X, Q
+    return 16.0 * (m * n * n - n ** 3 / 3.0), us * 1e-6
+
+
+def time_sliced_gemm(ctx, torch, stream, W):
+    """CUDA-event device time of the tensor-core kernel of the sliced GEMM at the workload's
+    effective-operator shape (prod_LR 3-index: M=chi, N=d chi, K=w chi), read through the
+    context's profiling hook, and of the whole sliced GEMM (slicing kernels included)."""
+    import ctypes as C
+    from mpsb200 import _lib
+    S, chi, d, w = W["slices"], W["chi"], W["d"], W["w"]
+    M, N, Kd = chi, d * chi, w * chi
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A = torch.randn(M * Kd, dtype=torch.complex128, device="cuda", generator=g)
+    B = torch.randn(Kd * N, dtype=torch.complex128, device="cuda", generator=g)
+    Cm = torch.zeros(M * N, dtype=torch.complex128, device="cuda")
+    torch.cuda.synchronize()
+    args = (ctx.h, M, N, Kd, C.c_void_p(A.data_ptr()), 1, M, 1, C.c_void_p(B.data_ptr()), 1, Kd, 0,
+            C.c_void_p(Cm.data_ptr()), 1, M, None, None, S)
+    reps = 10
+    us_all = _event_us(torch, stream, lambda: _lib.call("mpsb_op_zgemm", *args), reps, 2, ctx)
+    ctx.profile_read()
+    ctx.set_profiling(True)
+    for _ in range(reps):
+        _lib.call("mpsb_op_zgemm", *args)
+    ms, n = ctx.profile_read()
+    ctx.set_profiling(False)
+    del A, B, Cm
+    int8_ops = 2.0 * (S * (S + 1) // 2) * M * (2 * N) * (2 * Kd)
+    return {"M": M, "N": N, "K": Kd, "slices": S, "kernel_us": 1e3 * ms / n, "op_us": us_all,
+            "int8_ops": int8_ops, "complex_flops": 8.0 * M * N * Kd}
+
+
+def run_ours(args, rank, world, local_rank, dist):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import mpsb200 as K
+    from mpsb200 import _lib
+    from mpsb200 import models as GM
+
+    torch.cuda.set_device(local_rank)
+    W = WORKLOADS[args.workload]
+    pairs = W["pairs"]
+    split = W["slices"] > 0
+    ctx = K.Context(local_rank)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    b, p = workload_buffers(W, ctx, W["slices"])
+    dims = b.dims
+    wv = [1] + [W["w"]] * (W["na"] - 1) + [1]
+    fl = step_flops(dims, wv, W["d"])
+
+    # ---- warm-up of the measured arm, observables after every step
+    obs0 = b.observables(pairs)
+    obs = []
+    for _ in range(args.warmup):
+        b.step()
+        obs.append(b.observables(pairs))
+    ctx.sync()
+
+    # ---- the plain FP64 path on the same start, warm-up steps with observables
+    fp = None
+    if split:
+        ctx64 = K.Context(local_rank)
+        stream64 = torch.cuda.Stream()
+        ctx64.set_stream(stream64.cuda_stream)
+        b64, _ = workload_buffers(W, ctx64, 0)
+        obs64 = []
+        for _ in range(args.warmup):
+            b64.step()
+            obs64.append(b64.observables(pairs))
+        ctx64.sync()
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    l0 = ctx.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        torch.cuda.nvtx.range_push("rk4_step")
+        b.step()
+        torch.cuda.nvtx.range_pop()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = ctx.launches - l0
+    secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
+    value = job_rate(world, W["na"], args.steps, secs)
+    obs_end = b.observables(pairs)
+
+    check = {"trace_rho_end": float(np.real(obs_end[0])), "steps_compared": args.warmup}
+    if split:
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream64)
+        for _ in range(args.steps):
+            b64.step()
+        f1.record(stream64)
+        torch.cuda.synchronize()
+        secs64 = max_over_ranks(f0.elapsed_time(f1) / 1e3, dist)
+        value64 = job_rate(world, W["na"], args.steps, secs64)
+        obs64_end = b64.observables(pairs)
+        per_step = [obs_error(o, r) for o, r in zip(obs, obs64)]
+        err_end, scale_end = obs_error(obs_end, obs64_end)
+        ab = K.scal_prod(b.rho, b64.rho)
+        fid = abs(ab) ** 2 / (K.scal_prod(b.rho, b.rho).real * K.scal_prod(b64.rho, b64.rho).real)
+        fp = {"value": value64, "ms_per_step": 1e3 * secs64 / args.steps,
+              "split_vs_fp64": value / value64}
+        check.update({"obs_err_per_step_vs_fp64": [e for e, _ in per_step],
+                      "obs_scale": max(s for _, s in per_step) if per_step else None,
+                      "obs_rel_err_max_vs_fp64": max((e / s for e, s in per_step), default=None),
+                      "obs_err_after_%d_steps_vs_fp64" % (args.warmup + args.steps): err_end,
+                      "obs_rel_err_after_%d_steps_vs_fp64" % (args.warmup + args.steps): err_end / scale_end,
+                      "infidelity_vs_fp64_after_%d_steps" % (args.warmup + args.steps): 1.0 - fid})
+    # oracle golden values of the first steps (tests/golden), when present
+    gpath = os.path.join(ROOT, "tests", "golden", W["golden"])
+    if os.path.exists(gpath):
+        gz = np.load(gpath)
+        mi = 1 if W["chi0"] else 10      # steps between the fixture's records
+        recs = [obs0] + obs              # the measured arm after 0..warmup steps
+        errs = [obs_error(recs[i], (gz["tr"][i // mi], gz["see"][i // mi], gz["spm"][i // mi]))
+                for i in range(0, len(recs), mi) if i // mi < len(gz["tr"])]
+        if errs:
+            check["obs_rel_err_vs_oracle_golden"] = max(e / s for e, s in errs)
+            check["golden_steps"] = len(errs) - 1
+
+    # ---- end to end through the public API with host buffers: every step uploads the three
+    # generator MPOs from pinned host memory (the reference loop's update_L! refresh) and reads
+    # Tr(rho) back (the measurement of the example loop)
+    mpo_host = []
+    h2d = 0
+    for (con, delt, tt) in [(1, W["dt"] / 2, 0.0), (0, 1, W["dt"] / 2), (1, W["dt"] / 2, W["dt"])]:
+        sites = GM.construct_L_spin_model(p, con, delt, tt, W["w"])
+        pinned = []
+        for s in sites:
+            pt = torch.empty(s.size * 2, dtype=torch.float64, pin_memory=True)
+            arr = pt.numpy()
+            arr[:] = np.ascontiguousarray(s.ravel(order="F")).view(np.float64)
+            pinned.append((pt, arr.reshape(-1)))
+            h2d += s.size * 16
+        mpo_host.append(pinned)
+    ke = max(2, args.steps)
+
+    def e2e_step():
+        for mpo, pinned in zip(b.L, mpo_host):
+            for k, (_, arr) in enumerate(pinned):
+                _lib.call("mpsb_mpo_set_site", mpo.h, k + 1, arr.ctypes.data_as(C.POINTER(C.c_double)))
+        b.step()
+        K.scal_prod_no_conj(b.trace_fn, b.rho)
+
+    for _ in range(min(args.warmup, 2)):
+        e2e_step()
+    ctx.sync()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        e2e_step()
+    ctx.sync()
+    e2e_secs = max_over_ranks(time.perf_counter() - t0, dist)
+    e2e_value = job_rate(world, W["na"], ke, e2e_secs)
+
+    # ---- roofline of the dominant kernel
+    if split:
+        peak, src = load_peaks()
+        sg = time_sliced_gemm(ctx, torch, stream, W)
+        ach = sg["int8_ops"] / sg["kernel_us"] / 1e6
+        roofline = {"bound": "tensor", "pipe": "int8 (tcgen05 kind::i8)", "kernel": "ozgemm_kernel<%d>" % W["slices"],
+                    "achieved": ach, "peak": peak, "unit": "TOP/s", "frac": ach / peak, "peak_source": src,
+                    "traffic": None,
+                    "per_launch": "prod_LR 3-index shape M=%d N=%d K=%d: %d slice products x 2*M*2N*2K = %.3e int8 "
+                                  "ops in %.1f us (CUDA events around the kernel); whole sliced GEMM incl. slicing "
+                                  "%.1f us = %.1f complex TFLOP/s" % (
+                                      sg["M"], sg["N"], sg["K"], W["slices"] * (W["slices"] + 1) // 2,
+                                      sg["int8_ops"], sg["kernel_us"], sg["op_us"],
+                                      sg["complex_flops"] / sg["op_us"] / 1e6)}
+    else:
+        roofline = None
+    qm, qn = W["d"] * W["chi"], W["chi"]
+    qflops, qsecs = time_qr(ctx, torch, stream, qm, qn)
+    roofline_qr = {"bound": "fp64", "kernel": "qr_kernel (cluster Householder) + Q formation",
+                   "achieved": qflops / qsecs / 1e12, "unit": "TFLOP/s",
+                   "per_launch": "one QR of %d x %d: 16(mn^2 - n^3/3) = %.3e flops in %.1f us"
+                                 % (qm, qn, qflops, qsecs * 1e6)}
+    if roofline is None:
+        roofline = dict(roofline_qr, peak=None, frac=None, traffic=QR_TRAFFIC_BYTES if W["chi"] == 128 else None)
+
+    serving = None
+    if world == 1 and not args.no_serve:
+        serving = run_serving()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": ("complex128 operands, int8 slices x%d on the tensor pipe, FP64 QR/norms" % W["slices"]) if split
+        else "complex128",
+        "data": "synthetic (seeded random / all-down rho, waveguide Lindbladian)",
+        "config": config_dict(args, W),
+        "clocks": clocks,
+        "gpu_launches": int(launches),
+        "step_tflops": sum(fl.values()) * args.steps / secs * world / 1e12,
+        "step_flops": fl,
+        "fp64_path": fp,
+        "roofline": roofline,
+        "roofline_qr": roofline_qr,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16,
+                "steps": ke},
+        "check": check,
+        "serving": serving,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        model, cores = cpu_info()
+        value_cpu, t_sample, flx, mean_site = cpu_rate(W, 1)
+        line["cpu_baseline"] = {"value": value_cpu, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": "1 interior site-update (all its contractions and QRs in one RK4 step, "
+                                          "chi=%d) on the CPU oracle (NumPy/OpenBLAS, %s, %d threads): %.2f s; "
+                                          "chain rate scaled by interior/mean site flops (%.3g/%.3g)"
+                                          % (W["chi"], model, cores, t_sample, flx, mean_site)}
+    ctx.close()
+    if split:
+        ctx64.close()
+    return line
+
+
 def main():
     if "--op" in sys.argv:
         i = sys.argv.index("--op")
         return run_op(sys.argv[i + 1:])
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="precision", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream sample")
     args = ap.parse_args()

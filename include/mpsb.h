@@ -74,6 +74,13 @@ int mpsb_ctx_set_pipeline(mpsb_ctx* ctx, int enable);
  * (Complex{Float64}, or Complex{Float32} in its GPU examples,
  * examples/rydberg_density_matrix_gpu.jl:124-125); this setting has no direct counterpart. */
 int mpsb_ctx_set_precision(mpsb_ctx* ctx, int slices, int min_tiles);
+/* Device-time accounting of the sliced path's tensor-core GEMM kernel (no reference
+ * counterpart): while enabled, every eager launch of that kernel is bracketed by CUDA events;
+ * mpsb_ctx_profile_read waits for the context, returns the summed milliseconds and the number
+ * of launches since the last read, and clears them.  Launches inside captured graphs are not
+ * counted. */
+int mpsb_ctx_set_profiling(mpsb_ctx* ctx, int enable);
+int mpsb_ctx_profile_read(mpsb_ctx* ctx, double* ms, int64_t* launches);
 /* Kernel launches issued by this context since creation (for accounting). */
 int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out);
 

@@ -163,6 +163,10 @@ int mpsb_ctx_destroy(mpsb_ctx* ctx) {
   for (auto& kv : ctx->graphs_cache)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   cudaStreamSynchronize(ctx->side);
+  for (auto& p : ctx->prof_events) {
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
   ws_free(ctx->ws);
   ws_free(ctx->ws_side);
   for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
@@ -197,6 +201,32 @@ int mpsb_ctx_set_graphs(mpsb_ctx* ctx, int enable) {
 int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out) {
   if (!ctx || !out) return MPSB_ERR_INVALID_ARG;
   *out = ctx->ws.launches + ctx->ws_side.launches;
+  return MPSB_OK;
+}
+
+int mpsb_ctx_set_profiling(mpsb_ctx* ctx, int enable) {
+  if (!ctx) return MPSB_ERR_INVALID_ARG;
+  ctx->ws.prof = enable ? &ctx->prof_events : nullptr;
+  ctx->ws_side.prof = ctx->ws.prof;
+  return MPSB_OK;
+}
+
+int mpsb_ctx_profile_read(mpsb_ctx* ctx, double* ms, int64_t* launches) {
+  MPSB_TRY(bind(ctx));
+  if (!ms || !launches) return MPSB_ERR_INVALID_ARG;
+  MPSB_TRY(sync(ctx));
+  MPSB_CUDA_TRY(cudaStreamSynchronize(ctx->side));
+  double tot = 0.0;
+  for (auto& p : ctx->prof_events) {
+    float t = 0.f;
+    MPSB_CUDA_TRY(cudaEventElapsedTime(&t, p.first, p.second));
+    tot += t;
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  *ms = tot;
+  *launches = (int64_t)ctx->prof_events.size();
+  ctx->prof_events.clear();
   return MPSB_OK;
 }
 

@@ -557,8 +557,19 @@ int ozgemm_launch(const Gemm& g, int slices, void* scratch, size_t scratch_bytes
   const int64_t tiles = (Mpad / OZ_BM) * (NBpad / OZ_BN);
   if (tiles >= (int64_t(1) << 31)) return MPSB_ERR_UNSUPPORTED;
   count_launch(ws);
+  std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+  const bool timed = ws && ws->prof && !ws->capturing;
+  if (timed) {
+    MPSB_CUDA_TRY(cudaEventCreate(&ev.first));
+    MPSB_CUDA_TRY(cudaEventCreate(&ev.second));
+    MPSB_CUDA_TRY(cudaEventRecord(ev.first, s));
+  }
   fn<<<(unsigned)tiles, OZ_THREADS, smem_of(S), s>>>(ta, tb, P);
   MPSB_CUDA_TRY(cudaGetLastError());
+  if (timed) {
+    MPSB_CUDA_TRY(cudaEventRecord(ev.second, s));
+    ws->prof->push_back(ev);
+  }
   return MPSB_OK;
 }
 

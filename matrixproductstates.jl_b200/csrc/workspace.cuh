@@ -1,6 +1,9 @@
 // Device scratch owned by one context.  Buffers only grow; growth is refused while a CUDA
 // graph is being captured (the first, eager call of a step sizes everything).
 #pragma once
+#include <utility>
+#include <vector>
+
 #include "common.cuh"
 
 namespace mpsb {
@@ -18,6 +21,9 @@ struct Workspace {
   DevBuf named[16];       // per-sweep temporaries (see engine.cu)
   bool capturing = false;
   int64_t launches = 0;   // kernel launches issued (eager) or recorded (capture)
+  // when set (and not capturing), the sliced GEMM brackets its tensor-core kernel with a pair of
+  // CUDA events appended here, so its device time can be read apart from the slicing kernels
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* prof = nullptr;
 };
 
 inline void count_launch(Workspace* ws) {

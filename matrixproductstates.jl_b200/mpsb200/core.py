@@ -55,6 +55,17 @@ class Context:
         with that many slices per operand for GEMMs of at least ``min_tiles`` output tiles."""
         _lib.call("mpsb_ctx_set_precision", self.h, int(slices), int(min_tiles))
 
+    def set_profiling(self, enable):
+        """Bracket every eager launch of the sliced path's tensor-core GEMM kernel with CUDA
+        events (read with ``profile_read``)."""
+        _lib.call("mpsb_ctx_set_profiling", self.h, 1 if enable else 0)
+
+    def profile_read(self):
+        """(milliseconds, launches) of the tensor-core GEMM kernel since the last read."""
+        ms, n = C.c_double(), C.c_int64()
+        _lib.call("mpsb_ctx_profile_read", self.h, C.byref(ms), C.byref(n))
+        return ms.value, n.value
+
     def set_stream(self, stream_ptr):
         _lib.call("mpsb_ctx_set_stream", self.h, C.c_void_p(stream_ptr or 0))
 
