@@ -383,12 +383,22 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
   for (int l = 0; l < numv; ++l)
     if (Av[l]->na != na || Av[l]->d != d) return MPSB_ERR_DIMENSION;
   cudaStream_t st = ctx->stream;
-  std::vector<int64_t> dims = Ain->dims, cap(na + 1);
-  for (int k = 0; k <= na; ++k) {   // capacity of bond k: the dims rule bound with dlim
-    int64_t c = dlim, pl = 1, pr = 1;
-    for (int i = 0; i < k && pl < c; ++i) pl *= d;
-    for (int i = k; i < na && pr < c; ++i) pr *= d;
-    cap[k] = std::max<int64_t>(dims[k], std::min(c, std::min(pl, pr)));
+  auto bond_over_capacity = [](int b, int v, int64_t c) {   // cannot happen: cap bounds every pair
+    set_last_message("two-site compression: bond %d would be %d above its capacity %lld", b, v, (long long)c);
+    return MPSB_ERR_UNSUPPORTED;
+  };
+  std::vector<int64_t> dims = Ain->dims, cap(dims);
+  // capacity of bond k: the largest value the sweeps can give it.  A pair's new bond is at most
+  // min(bond[k-1] d, d bond[k+1], dlim), so the capacities are the smallest fixed point of
+  // cap[k] = max(guess[k], min(dlim, cap[k-1] d, d cap[k+1])) (monotone, bounded by
+  // max(guess, dlim)); a guess whose bonds exceed the dims rule raises its neighbours' capacity
+  // instead of being cut.
+  for (bool changed = true; changed;) {
+    changed = false;
+    for (int k = 1; k < na; ++k) {
+      const int64_t c = std::max<int64_t>(dims[k], std::min<int64_t>(dlim, std::min(cap[k - 1] * d, cap[k + 1] * d)));
+      if (c != cap[k]) { cap[k] = c; changed = true; }
+    }
   }
   auto DA = [&](int k) { return (int)A->dims[k]; };
   auto DL = [&](int l, int k) { return (int)Av[l]->dims[k]; };   // bond k of plain term l
@@ -519,9 +529,8 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
     for (int j = na - 2; j >= 0; --j) {
       MPSB_TRY(pair(j));
       MPSB_TRY(svd_pair(j, k));
-      // the scratch holds bond j+1 up to cap[j+1], which bounds the rule's result whenever the
-      // guess obeys the dims rule; a guess with larger bonds is clamped here, never overrun
-      dnew = std::min<int>(truncation_rule(S, k, svd_tol, dlim), (int)cap[j + 1]);
+      dnew = truncation_rule(S, k, svd_tol, dlim);
+      if (dnew > cap[j + 1]) return bond_over_capacity(j + 1, dnew, cap[j + 1]);
       if (dnew == 0) { set_last_message("two-site compression: zero pair tensor"); return MPSB_ERR_NONFINITE; }
       dims[j + 1] = dnew;
       const int n = d * (int)dims[j + 2];
@@ -536,9 +545,8 @@ int compress_two_site_sum(mpsb_ctx* ctx, const mpsb_mps* Ain, int numv, const cd
     for (int j = 0; j <= na - 2; ++j) {
       MPSB_TRY(pair(j));
       MPSB_TRY(svd_pair(j, k));
-      // the scratch holds bond j+1 up to cap[j+1], which bounds the rule's result whenever the
-      // guess obeys the dims rule; a guess with larger bonds is clamped here, never overrun
-      dnew = std::min<int>(truncation_rule(S, k, svd_tol, dlim), (int)cap[j + 1]);
+      dnew = truncation_rule(S, k, svd_tol, dlim);
+      if (dnew > cap[j + 1]) return bond_over_capacity(j + 1, dnew, cap[j + 1]);
       if (dnew == 0) { set_last_message("two-site compression: zero pair tensor"); return MPSB_ERR_NONFINITE; }
       dims[j + 1] = dnew;
       const int m = (int)dims[j] * d;

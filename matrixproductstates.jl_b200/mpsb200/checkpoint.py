@@ -17,6 +17,9 @@ import os
 import numpy as np
 
 _MPS_KEY = "__mps__"
+# MAT variable holding the exact shape of every non-MPS field (JSON), so that a size-1 array or a
+# 1 x n matrix reads back with the shape it was written with (MAT stores everything as >= 2-d)
+_MAT_SHAPES = "mpsb_field_shapes"
 
 
 def _mps_sites(v):
@@ -55,9 +58,9 @@ def write_data_file(filename, fields):
 
 def _write_mat(filename, fields):
     import scipy.io
-    out = {}
+    out, shapes = {}, {}
     for name, v in fields.items():
-        if not name.isidentifier():
+        if not name.isidentifier() or name == _MAT_SHAPES:
             raise ValueError("field name %r is not a MAT variable name" % name)
         sites = _mps_sites(v)
         if sites is not None:
@@ -67,6 +70,9 @@ def _write_mat(filename, fields):
             out[name] = cell
         else:
             out[name] = np.asarray(v)
+            if out[name].dtype.kind != "U":
+                shapes[name] = list(out[name].shape)
+    out[_MAT_SHAPES] = json.dumps(shapes)
     tmp = filename + ".tmp"
     with open(tmp, "wb") as f:
         scipy.io.savemat(f, out, format="5", do_compression=False, oned_as="row")
@@ -76,6 +82,7 @@ def _write_mat(filename, fields):
 def _read_mat(filename):
     import scipy.io
     raw = scipy.io.loadmat(filename, squeeze_me=False, chars_as_strings=True)
+    shapes = json.loads(str(raw.pop(_MAT_SHAPES)[0])) if _MAT_SHAPES in raw else None
     out, mps = {}, {}
     for name, a in raw.items():
         if name.startswith("__"):
@@ -85,17 +92,22 @@ def _read_mat(filename):
                          for c in a.ravel(order="F")]
         elif a.dtype.kind == "U":
             out[name] = str(a[0]) if a.size else ""
+        elif shapes is not None and name in shapes:
+            # only the 0-d / 1-d fields changed shape on the way out (to 1 x 1 / 1 x n)
+            shp = tuple(shapes[name])
+            b = a.reshape(shp) if a.size == int(np.prod(shp)) else a
+            out[name] = b.item() if b.ndim == 0 else b
         else:
-            # 1-d arrays go out as 1 x n rows: a row comes back 1-d, an n x 1 matrix stays 2-d
+            # a file written elsewhere (the reference's writer): 1 x 1 -> scalar, a 1 x n row -> 1-d
             out[name] = a.reshape(()).item() if a.size == 1 else (a.ravel() if a.ndim == 2 and a.shape[0] == 1 else a)
     return out, mps
 
 
 def read_data_file(filename, ctx=None, device=True):
     """Read a checkpoint.  MPS fields come back as device ``MPS`` objects on ``ctx`` (the
-    default context when None) if ``device``, else as lists of host site arrays; 0-d arrays
-    (1 x 1 in a MAT file) come back as Python scalars, MAT row vectors (how 1-d arrays are
-    written) as 1-d."""
+    default context when None) if ``device``, else as lists of host site arrays.  Every other
+    field comes back with the shape it was written with (0-d arrays as Python scalars); in a MAT
+    file written elsewhere, 1 x 1 values come back as scalars and 1 x n rows as 1-d arrays."""
     if _is_mat(filename):
         out, mps = _read_mat(filename)
         for name, sites in mps.items():

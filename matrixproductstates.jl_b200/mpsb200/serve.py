@@ -161,14 +161,22 @@ class Server:
                 if used + footprint(pending[0]) > self.budget:
                     break
                 job = pending.pop(0)
-                ctx = K.Context(self.device)
-                buf, r1, r2 = _start(job, ctx)
-                a = _Active(job, ctx, buf, time.perf_counter() - t0, r1=r1, r2=r2,
-                            rec={"p_coh": [], "jumps": []})
-                active.append(a)
-                used += footprint(job)
-                if on_admit is not None:
-                    on_admit(a)
+                ctx = a = None
+                try:   # a failure while setting the job up stays with the job
+                    ctx = K.Context(self.device)
+                    buf, r1, r2 = _start(job, ctx)
+                    a = _Active(job, ctx, buf, time.perf_counter() - t0, r1=r1, r2=r2,
+                                rec={"p_coh": [], "jumps": []})
+                    active.append(a)
+                    used += footprint(job)
+                    if on_admit is not None:
+                        on_admit(a)
+                except _lib.MpsbError as e:
+                    failed.append({"job_id": job.job_id, "step": -1, "error": str(e)})
+                    if a is not None and a in active:
+                        release(a)
+                    elif ctx is not None:
+                        ctx.close()
             if not active:
                 if pending:
                     time.sleep(max(0.0, min(0.01, pending[0].arrival - now)))

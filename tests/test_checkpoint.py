@@ -32,6 +32,37 @@ def test_checkpoint_round_trip_host(tmp_path, ext):
         assert raw["i_last"].shape == (1, 1)
 
 
+@pytest.mark.parametrize("ext", [".npz", ".mat"])
+def test_checkpoint_keeps_field_shapes(tmp_path, ext):
+    """Size-1 arrays and 1 x n matrices read back with their own shapes (a run checkpointed
+    before its second measurement holds exactly such observation arrays)."""
+    from mpsb200 import checkpoint as CK
+    f = str(tmp_path / ("obs" + ext))
+    fields = {"tr_rho": np.array([1.0 + 0j]), "see": np.array([[0.0, 1.0, 2.0, 3.0]]), "spm": np.zeros((1, 1), complex),
+              "col": np.arange(3.0).reshape(3, 1), "cube": np.arange(24.0).reshape(2, 3, 4), "n": 5, "x": 0.25}
+    CK.write_data_file(f, fields)
+    st = CK.read_data_file(f, device=False)
+    for k, v in fields.items():
+        assert np.shape(st[k]) == np.shape(v), k
+        assert np.array_equal(np.asarray(st[k]), np.asarray(v)), k
+    assert isinstance(st["n"], int) and isinstance(st["x"], float)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ext", [".npz", ".mat"])
+def test_resume_from_a_single_observation_row(gpu_ctx, tmp_path, ext):
+    """checkpoint_int < measure_int: the first checkpoint holds one observation row."""
+    from mpsb200 import drivers as GDR, models as GM
+    na, chi, dt = 6, 16, 0.005
+    pg = GM.WaveguideChain(na, gam_eg=0.1, omega=0.5, gam_phi=0.1)
+    b_ref, obs_ref = GDR.run_density(pg, chi, dt, 4, w=8, measure_int=2, ctx=gpu_ctx)
+    f = str(tmp_path / ("rho1_temp" + ext))
+    GDR.run_density(pg, chi, dt, 1, w=8, measure_int=2, ctx=gpu_ctx, checkpoint=f, checkpoint_int=1)
+    b, obs = GDR.run_density(pg, chi, dt, 4, w=8, measure_int=2, ctx=gpu_ctx, checkpoint=f)
+    assert all(np.array_equal(a, c) for a, c in zip(b.rho.sites(), b_ref.rho.sites()))
+    assert len(obs) == len(obs_ref)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("ext", [".npz", ".mat"])
 def test_resumed_density_run_equals_uninterrupted(gpu_ctx, tmp_path, ext):

@@ -188,6 +188,26 @@ def test_two_site_compression_matches_oracle(gpu_ctx, dlim, tol, sweeps):
     assert gd2 == dd2 and 1 - fidelity(got2.sites(), ref2) < 1e-10
 
 
+def test_two_site_guess_with_bonds_above_the_dims_rule(gpu_ctx):
+    """A guess whose bonds exceed the dims rule ([1,2,8,8,8,8,8,2,1] at d=2): the pairs next to
+    such a bond may need more than the rule allows, which the sweep scratch provides (nothing is
+    cut below the truncation rule); bonds and state equal the oracle's."""
+    import mpsb200 as K
+    na = 8
+    rng = np.random.default_rng(77)
+    A, dims = R.mpsrandom(na, 16, 2, rng)          # the full-rank target [1,2,4,8,16,8,4,2,1]
+    gdims = [1, 2, 8, 8, 8, 8, 8, 2, 1]
+    guess = [0.3 * R.crandn(rng, gdims[k], 2, gdims[k + 1]) for k in range(na)]
+    ident = [np.eye(2, dtype=np.complex128).reshape(1, 2, 1, 2)] * na
+    dd = list(gdims)
+    ref = R.compress_var_apply_H_two_site(R.copy_mps(guess), A, ident, 2, 1e-14, dd, 64)
+    gd = list(gdims)
+    got = K.compress_var_two_site(K.MPS.from_sites(guess, gpu_ctx), K.MPS.from_sites(A, gpu_ctx), 2, 1e-14, gd, 64)
+    assert gd == dd and got.dims == dd
+    assert all(x <= y for x, y in zip(gd, dims))
+    assert 1 - fidelity(got.sites(), A) < 1e-12 and 1 - fidelity(got.sites(), ref) < 1e-12
+
+
 @pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("with_h", [True, False])
 @pytest.mark.parametrize("dlim,tol", [(16, 1e-14), (5, 1e-6)])

@@ -34,6 +34,24 @@ def test_malformed_and_oversize_jobs_are_refused_at_admission():
     assert "steps" in reasons[3] and "dt" in reasons[4]
 
 
+def test_a_job_whose_setup_fails_is_recorded_and_the_stream_goes_on(monkeypatch):
+    """A library error while a job's context or buffers are created (here: a fake context whose
+    creation fails, so no device is needed) fails that job at step -1; the loop returns."""
+    from mpsb200 import _lib
+    from mpsb200 import serve as S
+
+    class FailingContext:
+        def __init__(self, device=0):
+            raise _lib.MpsbError(-4, "mpsb_ctx_create", "out of memory (injected)")
+
+    monkeypatch.setattr(S.K, "Context", FailingContext)
+    jobs = [S.Job("trajectory", 20, 16, 3, job_id=0), S.Job("density", 8, 16, 3, job_id=1)]
+    done, stats = S.Server(max_jobs=2, hbm_bytes=1 << 40).run(jobs)
+    assert done == [] and stats["refused"] == []
+    assert [(f["job_id"], f["step"]) for f in stats["failed"]] == [(0, -1), (1, -1)]
+    assert all("injected" in f["error"] for f in stats["failed"])
+
+
 @pytest.mark.gpu
 def test_a_failing_job_leaves_the_others_intact(gpu_ctx):
     """Fault injected from the host: one trajectory's Hamiltonian gets a NaN after admission.
