@@ -333,8 +333,10 @@ def load_peaks():
         return 2.0 * 1590.0, "2 x 1590 TFLOP/s bf16 of fallback (no MEASURED_PEAKS.json)"
 
 
-def workload_buffers(W, ctx, slices):
-    """Device buffers of the workload's density matrix on ctx, contractions at `slices`."""
+def workload_buffers(W, ctx, slices, start=None, perturb=0.0):
+    """Device buffers of the workload's density matrix on ctx, contractions at `slices`; start
+    "random" (chi0 > 0) or "down" (all-down product), every site entry scaled by
+    (1 + perturb N(0,1)) when perturb > 0."""
     import numpy as np
 
     import mpsb200 as K
@@ -342,12 +344,54 @@ def workload_buffers(W, ctx, slices):
     from mpsb200 import models as GM
     ctx.set_precision(slices)
     p = GM.WaveguideChain(W["na"], gam_eg=W["gam_eg"], omega=W["omega"], gam_phi=W["gam_phi"])
+    if start is None:
+        start = "random" if W["chi0"] else "down"
     rho = None
-    if W["chi0"]:
+    if start == "random":
         rho, _ = K.mpsrandom(W["na"], W["chi0"], W["d"], np.random.default_rng(W["seed"]), ctx)
         K.normalize_lo_(rho)
         rho, _ = K.expandmps(rho, W["chi"], ctx)
+    elif perturb:
+        rho, _ = K.mpsgroundstate(W["na"], W["chi"], W["d"], ctx)
+    if perturb:
+        rng = np.random.default_rng(5)
+        for k in range(rho.na):
+            s = rho.site(k)
+            rho.set_site(k, s * (1 + perturb * rng.standard_normal(s.shape)))
     return GDR.DensityBuffers(p, W["chi"], W["dt"], W["w"], ctx, rho), p
+
+
+def accuracy_arms(W, steps, local_rank):
+    """The split path against FP64 where it can be judged: (1) the FP64 path from the random
+    start perturbed by 1e-15 relative (the sensitivity of the truncated dynamics to rounding:
+    any two FP64 implementations differ by this much), (2) split and FP64 from the physical
+    all-down start at the same sizes, observables after every step."""
+    import mpsb200 as K
+    pairs = W["pairs"]
+    out = {}
+
+    def run(slices, start, perturb=0.0):
+        c = K.Context(local_rank)
+        try:
+            b, _ = workload_buffers(W, c, slices, start, perturb)
+            recs = []
+            for _ in range(steps):
+                b.step()
+                recs.append(b.observables(pairs))
+            c.sync()
+            del b
+        finally:
+            c.close()
+        return recs
+    if W["chi0"]:
+        ref = run(0, "random")
+        pert = run(0, "random", 1e-15)
+        out["fp64_envelope_rel_per_step"] = [e / s for e, s in (obs_error(a, b) for a, b in zip(pert, ref))]
+    d64 = run(0, "down")
+    dsp = run(W["slices"], "down")
+    out["down_start_obs_err_per_step_vs_fp64"] = [obs_error(a, b)[0] for a, b in zip(dsp, d64)]
+    out["down_start_trace_rho"] = [float(abs(r[0])) for r in d64]
+    return out
 
 
 def obs_error(a, b):
@@ -589,6 +633,8 @@ def run_ours(args, rank, world, local_rank, dist):
         err_end, scale_end = obs_error(obs_end, obs64_end)
         ab = K.scal_prod(b.rho, b64.rho)
         fid = abs(ab) ** 2 / (K.scal_prod(b.rho, b.rho).real * K.scal_prod(b64.rho, b64.rho).real)
+        del b64
+        ctx64.close()
         fp = {"value": value64, "ms_per_step": 1e3 * secs64 / args.steps,
               "split_vs_fp64": value / value64}
         check.update({"obs_err_per_step_vs_fp64": [e for e, _ in per_step],
@@ -670,6 +716,8 @@ def run_ours(args, rank, world, local_rank, dist):
     if roofline is None:
         roofline = dict(roofline_qr, peak=None, frac=None, traffic=QR_TRAFFIC_BYTES if W["chi"] == 128 else None)
 
+    if split and not args.no_accuracy:
+        check.update(accuracy_arms(W, args.warmup, local_rank))
     serving = None
     if world == 1 and not args.no_serve:
         serving = run_serving()
@@ -702,8 +750,6 @@ def run_ours(args, rank, world, local_rank, dist):
                                           "chain rate scaled by interior/mean site flops (%.3g/%.3g)"
                                           % (W["chi"], model, cores, t_sample, flx, mean_site)}
     ctx.close()
-    if split:
-        ctx64.close()
     return line
 
 
@@ -719,6 +765,7 @@ def main():
     ap.add_argument("--workload", default="precision", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream sample")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the envelope / physical-start arms")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -98,6 +98,27 @@ int mpsb_mps_site_ptr(const mpsb_mps* A, int site, void** dptr);
 /* dst .= copy.(src)  (examples/spin_model_quantum_trajectory_rk4.jl:130) */
 int mpsb_mps_copy(mpsb_mps* dst, const mpsb_mps* src);
 
+/* ---------------------------------------------------------------- batches of same-shape MPS
+ * The batched trajectory engine (no reference counterpart: the reference runs one trajectory per
+ * process, examples/spin_model_quantum_trajectory_rk4.jl:104-107).  A batch handle holds `batch`
+ * copies of one MPS shape back to back; every entry point that takes MPS / environment handles
+ * accepts batch handles of one common batch size (MPOs are shared by all copies) and runs each
+ * kernel over all copies at once.  Calls on batch handles, or on views of one copy, never split a
+ * GEMM's K, so a copy computes the same bits in a batch of any size.  Copies are 0-based. */
+int mpsb_mps_create_batch(mpsb_ctx* ctx, int na, int d, const int64_t* dims, int batch, mpsb_mps** out);
+int mpsb_env_create_batch(mpsb_ctx* ctx, int na, const int64_t* dims1, const int64_t* dims2,
+                          const int64_t* w /* na+1 or NULL */, int batch, mpsb_env** out);
+int mpsb_mps_batch(const mpsb_mps* A, int* batch);
+int mpsb_mps_set_site_copy(mpsb_mps* A, int copy, int site, const double* host);
+int mpsb_mps_get_site_copy(const mpsb_mps* A, int copy, int site, double* host);
+/* a handle on copy `copy` of a batch (shares its memory; destroy it before the batch) */
+int mpsb_mps_view(mpsb_mps* A, int copy, mpsb_mps** out);
+/* dst copy b <- srcs[which[b]] copy b (which[b] < 0 leaves copy b as it is): the per-trajectory
+ * choice of A = copy(A_coh) / copy(A_r) / copy(A_l), examples/...rk4.jl:130-178 */
+int mpsb_mps_select(mpsb_mps* dst, mpsb_mps* const* srcs, int nsrc, const int* which);
+/* normalize_lo! of every copy; no[b] = its norm^2 before scaling */
+int mpsb_normalize_lo_batch(mpsb_ctx* ctx, mpsb_mps* A, double* no);
+
 /* ---------------------------------------------------------------- MPO (Vector{Array{T,4}}) */
 int mpsb_mpo_create(mpsb_ctx* ctx, int na, int d, const int64_t* w /* na+1 */, mpsb_mpo** out);
 int mpsb_mpo_destroy(mpsb_mpo* O);

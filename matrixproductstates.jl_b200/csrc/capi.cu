@@ -169,6 +169,7 @@ int mpsb_ctx_destroy(mpsb_ctx* ctx) {
   }
   ws_free(ctx->ws);
   ws_free(ctx->ws_side);
+  if (ctx->vec.p) cudaFree(ctx->vec.p);
   for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
   cudaFree(ctx->d_scalars);
   cudaFreeHost(ctx->h_scalars);
@@ -249,12 +250,18 @@ int mpsb_ctx_set_pipeline(mpsb_ctx* ctx, int enable) {
 }
 
 // ---------------------------------------------------------------- MPS
-int mpsb_mps_create(mpsb_ctx* ctx, int na, int d, const int64_t* dims, mpsb_mps** out) {
+static void register_slab(mpsb_ctx* ctx, const void* base, int64_t total, int batch) {
+  const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+  ctx->slabs[b] = {b + (uintptr_t)(total * batch) * sizeof(cd), total};
+}
+
+static int mps_create(mpsb_ctx* ctx, int na, int d, const int64_t* dims, int batch, bool batched, mpsb_mps** out) {
   MPSB_TRY(bind(ctx));
-  if (!out || !dims || na < 1 || d < 1) return MPSB_ERR_INVALID_ARG;
+  if (!out || !dims || na < 1 || d < 1 || batch < 1 || batch > 65535) return MPSB_ERR_INVALID_ARG;
   if (dims[0] != 1 || dims[na] != 1) return MPSB_ERR_DIMENSION;
   mpsb_mps* A = new mpsb_mps();
   A->ctx = ctx; A->serial = ++g_serial; A->na = na; A->d = d;
+  A->batch = batch; A->batched = batched;
   A->dims.assign(dims, dims + na + 1);
   int64_t tot = 0;
   for (int k = 0; k < na; ++k) {
@@ -263,10 +270,30 @@ int mpsb_mps_create(mpsb_ctx* ctx, int na, int d, const int64_t* dims, mpsb_mps*
     tot += dims[k] * d * dims[k + 1];
   }
   A->total = tot;
-  int st = dev_alloc(&A->slab, tot);
+  int st = dev_alloc(&A->slab, tot * batch);
   if (st != MPSB_OK) { delete A; return st; }
-  cudaMemsetAsync(A->slab, 0, tot * sizeof(cd), ctx->stream);
+  cudaMemsetAsync(A->slab, 0, tot * batch * sizeof(cd), ctx->stream);
+  if (batched) register_slab(ctx, A->slab, tot, batch);
   *out = A;
+  return MPSB_OK;
+}
+
+int mpsb_mps_create(mpsb_ctx* ctx, int na, int d, const int64_t* dims, mpsb_mps** out) {
+  return mps_create(ctx, na, d, dims, 1, false, out);
+}
+
+int mpsb_mps_create_batch(mpsb_ctx* ctx, int na, int d, const int64_t* dims, int batch, mpsb_mps** out) {
+  return mps_create(ctx, na, d, dims, batch, true, out);
+}
+
+int mpsb_mps_view(mpsb_mps* A, int copy, mpsb_mps** out) {
+  if (!A || !out || copy < 0 || copy >= A->batch) return MPSB_ERR_INVALID_ARG;
+  mpsb_mps* V = new mpsb_mps(*A);
+  V->serial = ++g_serial;
+  V->batch = 1;
+  V->owns = false;
+  V->slab = A->slab + (int64_t)copy * A->total;
+  *out = V;
   return MPSB_OK;
 }
 
@@ -274,8 +301,51 @@ int mpsb_mps_destroy(mpsb_mps* A) {
   if (!A) return MPSB_ERR_INVALID_ARG;
   cudaSetDevice(A->ctx->device);
   cudaStreamSynchronize(A->ctx->stream);
-  cudaFree(A->slab);
+  if (A->owns) {
+    A->ctx->slabs.erase(reinterpret_cast<uintptr_t>(A->slab));
+    cudaFree(A->slab);
+  }
   delete A;
+  return MPSB_OK;
+}
+
+int mpsb_mps_batch(const mpsb_mps* A, int* batch) {
+  if (!A || !batch) return MPSB_ERR_INVALID_ARG;
+  *batch = A->batch;
+  return MPSB_OK;
+}
+
+int mpsb_mps_set_site_copy(mpsb_mps* A, int copy, int site, const double* host) {
+  if (!A || !host || site < 1 || site > A->na || copy < 0 || copy >= A->batch) return MPSB_ERR_INVALID_ARG;
+  MPSB_TRY(bind(A->ctx));
+  return upload(A->ctx, A->site(site - 1) + (int64_t)copy * A->total, host, A->site_elems(site - 1));
+}
+
+int mpsb_mps_get_site_copy(const mpsb_mps* A, int copy, int site, double* host) {
+  if (!A || !host || site < 1 || site > A->na || copy < 0 || copy >= A->batch) return MPSB_ERR_INVALID_ARG;
+  MPSB_TRY(bind(A->ctx));
+  return download(A->ctx, host, A->site(site - 1) + (int64_t)copy * A->total, A->site_elems(site - 1));
+}
+
+int mpsb_mps_select(mpsb_mps* dst, mpsb_mps* const* srcs, int nsrc, const int* which) {
+  if (!dst || !srcs || !which || nsrc < 1) return MPSB_ERR_INVALID_ARG;
+  for (int i = 0; i < nsrc; ++i) {
+    if (!srcs[i]) return MPSB_ERR_INVALID_ARG;
+    if (srcs[i]->dims != dst->dims || srcs[i]->d != dst->d || srcs[i]->batch != dst->batch) return MPSB_ERR_DIMENSION;
+  }
+  MPSB_TRY(bind(dst->ctx));
+  const int B = dst->batch;
+  for (int b = 0; b < B;) {
+    const int w = which[b];
+    if (w >= nsrc) return MPSB_ERR_INVALID_ARG;
+    int e = b + 1;
+    while (e < B && which[e] == w) ++e;   // one copy per run of equal sources
+    if (w >= 0 && srcs[w] != dst)
+      MPSB_CUDA_TRY(cudaMemcpyAsync(dst->slab + (int64_t)b * dst->total, srcs[w]->slab + (int64_t)b * dst->total,
+                                    (size_t)(e - b) * dst->total * sizeof(cd), cudaMemcpyDeviceToDevice,
+                                    dst->ctx->stream));
+    b = e;
+  }
   return MPSB_OK;
 }
 
@@ -307,9 +377,10 @@ int mpsb_mps_site_ptr(const mpsb_mps* A, int site, void** dptr) {
 
 int mpsb_mps_copy(mpsb_mps* dst, const mpsb_mps* src) {
   if (!dst || !src) return MPSB_ERR_INVALID_ARG;
-  if (dst->na != src->na || dst->d != src->d || dst->dims != src->dims) return MPSB_ERR_DIMENSION;
+  if (dst->na != src->na || dst->d != src->d || dst->dims != src->dims || dst->batch != src->batch)
+    return MPSB_ERR_DIMENSION;
   MPSB_TRY(bind(dst->ctx));
-  MPSB_CUDA_TRY(cudaMemcpyAsync(dst->slab, src->slab, src->total * sizeof(cd), cudaMemcpyDeviceToDevice,
+  MPSB_CUDA_TRY(cudaMemcpyAsync(dst->slab, src->slab, src->total * src->batch * sizeof(cd), cudaMemcpyDeviceToDevice,
                                 dst->ctx->stream));
   return MPSB_OK;
 }
@@ -358,12 +429,13 @@ int mpsb_mpo_get_site(const mpsb_mpo* O, int site, double* host) {
 }
 
 // ---------------------------------------------------------------- environments
-int mpsb_env_create(mpsb_ctx* ctx, int na, const int64_t* dims1, const int64_t* dims2, const int64_t* w,
-                    mpsb_env** out) {
+static int env_create(mpsb_ctx* ctx, int na, const int64_t* dims1, const int64_t* dims2, const int64_t* w, int batch,
+                      bool batched, mpsb_env** out) {
   MPSB_TRY(bind(ctx));
-  if (!out || !dims1 || !dims2 || na < 1) return MPSB_ERR_INVALID_ARG;
+  if (!out || !dims1 || !dims2 || na < 1 || batch < 1 || batch > 65535) return MPSB_ERR_INVALID_ARG;
   mpsb_env* E = new mpsb_env();
   E->ctx = ctx; E->serial = ++g_serial; E->na = na; E->three = (w != nullptr);
+  E->batch = batch; E->batched = batched;
   int64_t tot = 0;
   for (int e = 0; e <= na; ++e) {
     bool end = (e == 0 || e == na);
@@ -374,22 +446,34 @@ int mpsb_env_create(mpsb_ctx* ctx, int na, const int64_t* dims1, const int64_t* 
     tot += E->d1.back() * E->w.back() * E->d2.back();
   }
   E->total = tot;
-  int st = dev_alloc(&E->slab, tot);
+  int st = dev_alloc(&E->slab, tot * batch);
   if (st != MPSB_OK) { delete E; return st; }
-  cudaMemsetAsync(E->slab, 0, tot * sizeof(cd), ctx->stream);
+  cudaMemsetAsync(E->slab, 0, tot * batch * sizeof(cd), ctx->stream);
   count_launch(&ctx->ws);
-  set_value(E->entry(0), cmk(1.0, 0.0), ctx->stream);
+  set_value_strided(E->entry(0), tot, batch, cmk(1.0, 0.0), ctx->stream);
   count_launch(&ctx->ws);
-  set_value(E->entry(na), cmk(1.0, 0.0), ctx->stream);
+  set_value_strided(E->entry(na), tot, batch, cmk(1.0, 0.0), ctx->stream);
   MPSB_CUDA_TRY(cudaGetLastError());
+  if (batched) register_slab(ctx, E->slab, tot, batch);
   *out = E;
   return MPSB_OK;
+}
+
+int mpsb_env_create(mpsb_ctx* ctx, int na, const int64_t* dims1, const int64_t* dims2, const int64_t* w,
+                    mpsb_env** out) {
+  return env_create(ctx, na, dims1, dims2, w, 1, false, out);
+}
+
+int mpsb_env_create_batch(mpsb_ctx* ctx, int na, const int64_t* dims1, const int64_t* dims2, const int64_t* w,
+                          int batch, mpsb_env** out) {
+  return env_create(ctx, na, dims1, dims2, w, batch, true, out);
 }
 
 int mpsb_env_destroy(mpsb_env* E) {
   if (!E) return MPSB_ERR_INVALID_ARG;
   cudaSetDevice(E->ctx->device);
   cudaStreamSynchronize(E->ctx->stream);
+  E->ctx->slabs.erase(reinterpret_cast<uintptr_t>(E->slab));
   cudaFree(E->slab);
   delete E;
   return MPSB_OK;
@@ -498,6 +582,23 @@ int mpsb_norm_lo(mpsb_ctx* ctx, const mpsb_mps* A, double* no) {
   MPSB_CUDA_TRY(cudaMemcpyAsync(no, ctx->d_scalars, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   MPSB_TRY(sync(ctx));
   if (!(*no == *no) || *no > 1e300) return MPSB_ERR_NONFINITE;
+  return MPSB_OK;
+}
+
+int mpsb_normalize_lo_batch(mpsb_ctx* ctx, mpsb_mps* A, double* no) {
+  MPSB_TRY(bind(ctx));
+  if (!A || !no) return MPSB_ERR_INVALID_ARG;
+  const int s = A->na - 1, B = A->batch;
+  MPSB_TRY(devbuf_ensure(nullptr, ctx->vec, (size_t)B * sizeof(double)));
+  double* dn = static_cast<double*>(ctx->vec.p);
+  count_launch(&ctx->ws);
+  MPSB_TRY(norm2_batched(A->site(s), A->site_elems(s), A->total, B, dn, ctx->stream));
+  count_launch(&ctx->ws);
+  MPSB_TRY(scale_by_rsqrt_batched(A->site(s), A->site_elems(s), A->total, B, dn, ctx->stream));
+  MPSB_CUDA_TRY(cudaMemcpyAsync(no, dn, (size_t)B * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  MPSB_TRY(sync(ctx));
+  for (int b = 0; b < B; ++b)
+    if (!(no[b] == no[b]) || no[b] > 1e300) return MPSB_ERR_NONFINITE;
   return MPSB_OK;
 }
 

@@ -87,6 +87,8 @@ int gemm_launch(const Gemm& g, Workspace* ws, cudaStream_t s);
 // Small-K "apply a local MPO tensor" contraction:
 //   Out[x, m, y] = sum_k In[x, k, y] * Op[k, m]   with k = (k1, k2), m = (m1, m2) split indices.
 struct MpoApply {
+  int batch = 1;                  // problems, operands offset by the *_b strides
+  int64_t in_b = 0, op_b = 0, out_b = 0;
   int X = 0, Y = 0;               // free extents
   int K1 = 0, K2 = 0, M1 = 0, M2 = 0;
   const cd* in = nullptr;  int64_t in_x = 0, in_k1 = 0, in_k2 = 0, in_y = 0;
@@ -108,6 +110,8 @@ struct Workspace;
 // Q (and R) of each problem; uses the workspace's QR scratch (V, tau, V^H V, T V1^H)
 int qr_launch(const QrProblem& p, Workspace* ws, cudaStream_t s);
 bool qr_supported(int m, int n);
+// true when one cluster factorises an m x n problem (batched problems run in one launch)
+bool qr_batch_supported(int m, int n);
 // thin SVD X = U diag(S) V^H by one-sided Jacobi (S on the host, descending)
 int svd_launch(int m, int n, const cd* X, int64_t x_r, int64_t x_c, cd* U, int64_t u_r, int64_t u_c, double* S,
                cd* V, int64_t v_r, int64_t v_c, Workspace* ws, cudaStream_t st);

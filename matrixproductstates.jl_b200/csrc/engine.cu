@@ -18,12 +18,64 @@ struct SplitScope {
   ~SplitScope() { c->split_on = prev; }
 };
 
+// A scratch slot of `bytes` per copy: in a batched call it holds ctx->batch copies, registered
+// with the copy stride cap / batch so that every kernel finds copy b of any pointer into it.
 int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out) {
   DevBuf& b = ctx->ws.named[s];
   void* before = b.p;
-  MPSB_TRY(devbuf_ensure(&ctx->ws, b, bytes));
-  if (b.p != before) ctx->ws_generation++;
+  const size_t B = (size_t)std::max(1, ctx->batch);
+  MPSB_TRY(devbuf_ensure(&ctx->ws, b, bytes * B));
+  if (b.p != before) {
+    ctx->ws_generation++;
+    if (before) ctx->slabs.erase(reinterpret_cast<uintptr_t>(before));
+  }
+  const uintptr_t base = reinterpret_cast<uintptr_t>(b.p);
+  if (B > 1) ctx->slabs[base] = {base + b.cap, (int64_t)(b.cap / sizeof(cd) / B)};
+  else ctx->slabs.erase(base);
   *out = static_cast<cd*>(b.p);
+  return MPSB_OK;
+}
+
+// The copies of a batched call: every MPS and environment handle of the call must hold the same
+// number of copies; a handle created as part of a batch (or a view of one copy) puts the call in
+// batched mode (no split-K, no sliced path), so that a copy computes the same bits in a batch of
+// any size.  While alive, kernels of the context run ctx->batch copies.
+struct BatchScope {
+  mpsb_ctx* c;
+  int prev;
+  bool prev_ns, prev_ns_side, prev_split;
+  BatchScope(mpsb_ctx* ctx, int B, bool batched)
+      : c(ctx), prev(ctx->batch), prev_ns(ctx->ws.no_splitk), prev_ns_side(ctx->ws_side.no_splitk),
+        prev_split(ctx->split_on) {
+    c->batch = B;
+    c->ws.no_splitk = c->ws_side.no_splitk = batched;
+    if (batched) c->split_on = false;
+  }
+  ~BatchScope() {
+    c->batch = prev;
+    c->ws.no_splitk = prev_ns;
+    c->ws_side.no_splitk = prev_ns_side;
+    c->split_on = prev_split;
+  }
+};
+
+static int call_batch(std::initializer_list<const mpsb_mps*> mps, std::initializer_list<const mpsb_env*> envs,
+                      int* B, bool* batched) {
+  *B = -1;
+  *batched = false;
+  for (const mpsb_mps* m : mps) {
+    if (!m) continue;
+    if (*B < 0) *B = m->batch;
+    if (m->batch != *B) return MPSB_ERR_DIMENSION;
+    *batched = *batched || m->batched;
+  }
+  for (const mpsb_env* e : envs) {
+    if (!e) continue;
+    if (*B < 0) *B = e->batch;
+    if (e->batch != *B) return MPSB_ERR_DIMENSION;
+    *batched = *batched || e->batched;
+  }
+  if (*B < 0) *B = 1;
   return MPSB_OK;
 }
 
@@ -32,7 +84,14 @@ static bool split_worth(const mpsb_ctx* ctx, const Gemm& g) {
   return tiles >= ctx->split_min_tiles && g.K >= 16;
 }
 
-int run_gemm(mpsb_ctx* ctx, const Gemm& g) {
+int run_gemm(mpsb_ctx* ctx, const Gemm& g0) {
+  Gemm g = g0;
+  if (ctx->batch > 1 && g.batch == 1) {
+    g.batch = ctx->batch;
+    g.a_b = ctx->stride_of(g.A);
+    g.b_b = ctx->stride_of(g.B);
+    g.c_b = ctx->stride_of(g.C);
+  }
   if (ctx->split_on && ozgemm_supported(g, ctx->split_slices) && split_worth(ctx, g)) {
     void* before_oz = ctx->ws.oz.p;
     MPSB_TRY(devbuf_ensure(&ctx->ws, ctx->ws.oz, ozgemm_scratch_bytes(g, ctx->split_slices)));
@@ -45,7 +104,14 @@ int run_gemm(mpsb_ctx* ctx, const Gemm& g) {
   return st;
 }
 
-static inline int run_mpo(mpsb_ctx* ctx, const MpoApply& a, int64_t k1, int64_t k2, int64_t m1, int64_t m2) {
+static inline int run_mpo(mpsb_ctx* ctx, const MpoApply& a0, int64_t k1, int64_t k2, int64_t m1, int64_t m2) {
+  MpoApply a = a0;
+  if (ctx->batch > 1) {
+    a.batch = ctx->batch;
+    a.in_b = ctx->stride_of(a.in);
+    a.op_b = ctx->stride_of(a.op);
+    a.out_b = ctx->stride_of(a.out);
+  }
   count_launch(&ctx->ws);
   return mpo_apply_launch_strided(a, k1, k2, m1, m2, ctx->stream);
 }
@@ -183,11 +249,29 @@ int op_update_lenv(mpsb_ctx* ctx, const cd* A0, const cd* AL, cd* env, int lead,
 
 // QR through the context's workspace; a reallocated QR or split-K scratch (the blocked QR's
 // trailing GEMMs may split K) invalidates captured graphs
-int run_qr(mpsb_ctx* ctx, const QrProblem& p) {
+int run_qr(mpsb_ctx* ctx, const QrProblem& p0) {
+  QrProblem p = p0;
+  int loops = 1;
+  if (ctx->batch > 1 && p.batch == 1) {
+    p.x_b = ctx->stride_of(p.X);
+    p.q_b = ctx->stride_of(p.Q);
+    p.r_b = p.R ? ctx->stride_of(p.R) : 0;
+    if (qr_batch_supported(p.m, p.n)) p.batch = ctx->batch;
+    else loops = ctx->batch;   // shapes beyond one cluster: one copy after the other
+  }
   void* before = ctx->ws.qr.p;
   void* before_sk = ctx->ws.splitk.p;
-  count_launch(&ctx->ws);
-  int st = qr_launch(p, &ctx->ws, ctx->stream);
+  int st = MPSB_OK;
+  for (int b = 0; b < loops && st == MPSB_OK; ++b) {
+    QrProblem q = p;
+    if (loops > 1) {
+      q.X += b * p.x_b;
+      q.Q += b * p.q_b;
+      if (q.R) q.R += b * p.r_b;
+    }
+    count_launch(&ctx->ws);
+    st = qr_launch(q, &ctx->ws, ctx->stream);
+  }
   if (ctx->ws.qr.p != before || ctx->ws.splitk.p != before_sk) ctx->ws_generation++;
   return st;
 }
@@ -221,6 +305,7 @@ static int same_dims(const mpsb_mps* a, const mpsb_mps* b) {
 
 int set_boundary(mpsb_ctx* ctx, cd* p, cd v) {
   count_launch(&ctx->ws);
+  if (ctx->batch > 1) return set_value_strided(p, ctx->stride_of(p), ctx->batch, v, ctx->stream);
   return set_value(p, v, ctx->stream);
 }
 
@@ -378,6 +463,12 @@ int compress_sum_var_apply_H(mpsb_ctx* ctx, bool right, mpsb_mps* A0, mpsb_env* 
   if (!ctx || !A0 || !envop || !Ain || !coef || !A || !H || numv < 1) return MPSB_ERR_INVALID_ARG;
   MPSB_TRY(sum_var_check(A0, env, envop, Ain, numv, A, H));
   SplitScope scope(ctx);
+  int B;
+  bool batched;
+  MPSB_TRY(call_batch({A0, Ain}, {envop}, &B, &batched));
+  for (int l = 0; l < numv; ++l)
+    if (A[l]->batch != B || (l < numv - 1 && env[l]->batch != B)) return MPSB_ERR_DIMENSION;
+  BatchScope bscope(ctx, B, batched);
   SweepScratch s;
   MPSB_TRY(sweep_scratch(ctx, A0, H, numv - 1, s));
   MPSB_TRY(sum_var_init(ctx, right, env, envop, Ain, coef, numv, A, H, s, nullptr));
@@ -397,6 +488,10 @@ int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mps
   if (!ctx || !A0 || !envop || !Ain || !A || !H || maxsweeps < 0) return MPSB_ERR_INVALID_ARG;
   if (!same_dims(A0, Ain) || !same_dims(A0, A) || !envop->three || H->na != A0->na) return MPSB_ERR_DIMENSION;
   SplitScope scope(ctx);
+  int B;
+  bool batched;
+  MPSB_TRY(call_batch({A0, Ain, A}, {envop}, &B, &batched));
+  BatchScope bscope(ctx, B, batched);
   const int na = A0->na, d = A0->d;
   for (int k = 0; k <= na; ++k)
     if (envop->d1[k] != A0->dims[k] || envop->d2[k] != A0->dims[k] || envop->w[k] != H->w[k]) return MPSB_ERR_DIMENSION;
@@ -439,6 +534,12 @@ int compress_sum_var_full(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const cd
   if (!ctx || !A0 || !coef || !A || numv < 1 || maxsweeps < 0) return MPSB_ERR_INVALID_ARG;
   const bool hasH = H != nullptr;
   SplitScope scope(ctx);
+  int B;
+  bool batched;
+  MPSB_TRY(call_batch({A0}, {hasH ? envop : nullptr}, &B, &batched));
+  for (int l = 0; l < numv; ++l)
+    if (A[l] && A[l]->batch != B) return MPSB_ERR_DIMENSION;
+  BatchScope bscope(ctx, B, batched);
   if (hasH && !envop) return MPSB_ERR_INVALID_ARG;
   const int np = hasH ? numv - 1 : numv;
   if (np < 1) {   // the reference indexes the first plain term unconditionally
@@ -677,11 +778,15 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
   if (!ctx || !H1 || !H2 || !H3 || !psi0 || !psi || !psi1 || !psi2 || !psi3 || !env1 || !env2 || !env3 || !envop)
     return MPSB_ERR_INVALID_ARG;
   SplitScope scope(ctx);
+  int B;
+  bool batched;
+  MPSB_TRY(call_batch({psi0, psi, psi1, psi2, psi3}, {env1, env2, env3, envop}, &B, &batched));
+  BatchScope bscope(ctx, B, batched);
   if (!ctx->graphs)
     return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
   int64_t dtbits;
   std::memcpy(&dtbits, &dt, sizeof(dt));
-  std::vector<int64_t> key = {ctx->pipeline ? 2 : 1, ctx->split_slices, ctx->split_min_tiles, dtbits, H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial,
+  std::vector<int64_t> key = {ctx->pipeline ? 2 : 1, ctx->split_slices, ctx->split_min_tiles, B, dtbits, H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial,
                               psi1->serial, psi2->serial, psi3->serial, env1->serial, env2->serial,
                               env3->serial, envop->serial};
   auto& ent = ctx->graphs_cache[key];

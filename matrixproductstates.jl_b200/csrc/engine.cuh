@@ -26,6 +26,24 @@ struct mpsb_ctx {
   int split_slices = 0;
   int split_min_tiles = 64;
   bool split_on = false;       // set while a sweep entry point issues its contractions
+  // batched calls: every MPS / environment handle of the call holds `batch` copies of the same
+  // shape back to back, and each kernel runs all copies at once.  The registry maps the base of
+  // every batched slab (handles and scratch slots) to its end and its copy stride (elements);
+  // a pointer outside every registered slab (an MPO) is shared by all copies.
+  int batch = 1;
+  mpsb::DevBuf vec;   // per-copy results of batched calls (norms)
+  struct Slab {
+    uintptr_t end;
+    int64_t stride;
+  };
+  std::map<uintptr_t, Slab> slabs;
+  int64_t stride_of(const void* p) const {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    auto it = slabs.upper_bound(a);
+    if (it == slabs.begin()) return 0;
+    --it;
+    return a < it->second.end ? it->second.stride : 0;
+  }
   int64_t ws_generation = 0;   // bumped whenever a scratch buffer is reallocated
   double* d_scalars = nullptr; // small device scratch for norms (64 doubles)
   double* h_scalars = nullptr; // pinned host mirror
@@ -45,6 +63,9 @@ struct mpsb_ctx {
 struct mpsb_mps {
   mpsb_ctx* ctx = nullptr;
   int64_t serial = 0;
+  int batch = 1;          // copies in the slab (copy stride = total)
+  bool batched = false;   // a batch handle or a view of one copy: calls run in batched mode
+  bool owns = true;       // false for a view (the slab belongs to the batch handle)
   int na = 0, d = 0;
   std::vector<int64_t> dims;   // na+1
   std::vector<int64_t> off;    // element offset of each site
@@ -69,6 +90,8 @@ struct mpsb_mpo {
 struct mpsb_env {
   mpsb_ctx* ctx = nullptr;
   int64_t serial = 0;
+  int batch = 1;          // copies in the slab (copy stride = total)
+  bool batched = false;
   int na = 0;
   bool three = false;
   std::vector<int64_t> d1, d2, w;  // na+1 each (w all 1 for 2-index)

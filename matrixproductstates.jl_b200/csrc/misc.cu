@@ -1,4 +1,5 @@
 // Small kernels of the sweeps: boundary-env writes, FP64 norms, rescaling, local_exp.
+#include <algorithm>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -76,6 +77,32 @@ __global__ void local_exp_kernel(const cd* __restrict__ A0, const cd* __restrict
   if (threadIdx.x == 0) *out = total;
 }
 
+__global__ void set_value_strided_kernel(cd* p, int64_t stride, int batch, cd v) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < batch; b += gridDim.x * blockDim.x) p[b * stride] = v;
+}
+
+// one CTA per copy; the same reduction tree as norm2_kernel
+__global__ void norm2_batched_kernel(const cd* __restrict__ x0, int64_t n, int64_t stride, double* out) {
+  __shared__ double red[1024];
+  const cd* x = x0 + (int64_t)blockIdx.x * stride;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s = fma(x[i].x, x[i].x, fma(x[i].y, x[i].y, s));
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+__global__ void scale_by_rsqrt_batched_kernel(cd* x0, int64_t n, int64_t stride, const double* no) {
+  cd* x = x0 + (int64_t)blockIdx.y * stride;
+  const double s = sqrt(no[blockIdx.y]);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = cmk(x[i].x / s, x[i].y / s);
+}
+
 __global__ void copy_kernel(cd* dst, const cd* src, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     dst[i] = src[i];
@@ -92,6 +119,27 @@ int grid_for(int64_t n) {
 
 int set_value(cd* p, cd v, cudaStream_t s) {
   set_value_kernel<<<1, 1, 0, s>>>(p, v);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  return MPSB_OK;
+}
+
+int set_value_strided(cd* p, int64_t stride, int batch, cd v, cudaStream_t s) {
+  set_value_strided_kernel<<<(batch + 255) / 256, 256, 0, s>>>(p, stride, batch, v);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  return MPSB_OK;
+}
+
+int norm2_batched(const cd* x, int64_t n, int64_t stride, int batch, double* out, cudaStream_t s) {
+  if (batch < 1 || batch > 65535) return MPSB_ERR_UNSUPPORTED;
+  norm2_batched_kernel<<<batch, 1024, 0, s>>>(x, n, stride, out);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  return MPSB_OK;
+}
+
+int scale_by_rsqrt_batched(cd* x, int64_t n, int64_t stride, int batch, const double* no, cudaStream_t s) {
+  if (batch < 1 || batch > 65535) return MPSB_ERR_UNSUPPORTED;
+  const int gx = (int)std::min<int64_t>((n + 255) / 256, 64);
+  scale_by_rsqrt_batched_kernel<<<dim3(gx, batch), 256, 0, s>>>(x, n, stride, no);
   MPSB_CUDA_TRY(cudaGetLastError());
   return MPSB_OK;
 }

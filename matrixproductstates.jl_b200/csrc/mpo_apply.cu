@@ -30,13 +30,14 @@ __global__ void __launch_bounds__(NT) mpo_apply_kernel(MpoParams P) {
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * TX;
   const int y = blockIdx.y;
+  const int64_t bz = blockIdx.z;
 
   for (int e = tid; e < K * M; e += NT) {
     int m = e % M, k = e / M;
     int k1 = k % a.K1, k2 = k / a.K1, m1 = m % a.M1, m2 = m / a.M1;
-    opS[e] = a.op[k1 * P.op_k1 + k2 * P.op_k2 + m1 * P.op_m1 + m2 * P.op_m2];
+    opS[e] = a.op[bz * a.op_b + k1 * P.op_k1 + k2 * P.op_k2 + m1 * P.op_m1 + m2 * P.op_m2];
   }
-  const cd* in = a.in + (int64_t)y * a.in_y;
+  const cd* in = a.in + bz * a.in_b + (int64_t)y * a.in_y;
   for (int e = tid; e < K * TX; e += NT) {
     int x, k;
     if (P.k1_fast) { k = e % K; x = e / K; }
@@ -50,7 +51,7 @@ __global__ void __launch_bounds__(NT) mpo_apply_kernel(MpoParams P) {
   const int x = tid % TX, mg = tid / TX;   // 4 m-groups
   const int gx = x0 + x;
   const bool use_beta = (a.beta.x != 0.0) || (a.beta.y != 0.0);
-  cd* out = a.out + (int64_t)y * a.out_y;
+  cd* out = a.out + bz * a.out_b + (int64_t)y * a.out_y;
   for (int mb = mg * 8; mb < M; mb += 32) {
     cd acc[8];
 #pragma unroll
@@ -85,13 +86,13 @@ int mpo_apply_launch_strided(const MpoApply& a, int64_t op_k1, int64_t op_k2, in
   if (K <= 0 || M <= 0) return MPSB_ERR_DIMENSION;
   size_t smem = (size_t)(K * M + K * TX) * sizeof(cd);
   if (smem > 200 * 1024) return MPSB_ERR_UNSUPPORTED;
-  if (a.Y > 65535) return MPSB_ERR_UNSUPPORTED;
+  if (a.Y > 65535 || a.batch < 1 || a.batch > 65535) return MPSB_ERR_UNSUPPORTED;
   MPSB_TRY(ensure_kernel_attrs((const void*)mpo_apply_kernel, 200 * 1024));
   MpoParams P;
   P.a = a;
   P.op_k1 = op_k1; P.op_k2 = op_k2; P.op_m1 = op_m1; P.op_m2 = op_m2;
   P.k1_fast = (a.in_k1 == 1) && (a.in_x != 1);
-  dim3 grid((a.X + TX - 1) / TX, a.Y);
+  dim3 grid((a.X + TX - 1) / TX, a.Y, a.batch);
   mpo_apply_kernel<<<grid, NT, smem, s>>>(P);
   MPSB_CUDA_TRY(cudaGetLastError());
   return MPSB_OK;

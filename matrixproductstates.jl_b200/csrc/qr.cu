@@ -923,6 +923,11 @@ bool blocked_ok(int m, int n) {
 
 }  // namespace
 
+bool qr_batch_supported(int m, int n) {
+  Choice ch;
+  return m >= n && n >= 1 && n <= 512 && choose(m, n, ch);
+}
+
 bool qr_supported(int m, int n) {
   Choice ch;
   return m >= n && n >= 1 && n <= 512 && (choose(m, n, ch) || blocked_ok(m, n));

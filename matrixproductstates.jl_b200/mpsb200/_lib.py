@@ -47,6 +47,14 @@ SIGNATURES = {
     "mpsb_mps_get_site": ([_vp, _i, _pd], _i),
     "mpsb_mps_site_ptr": ([_vp, _i, _pvp], _i),
     "mpsb_mps_copy": ([_vp, _vp], _i),
+    "mpsb_mps_create_batch": ([_vp, _i, _i, _pi64, _i, _pvp], _i),
+    "mpsb_env_create_batch": ([_vp, _i, _pi64, _pi64, _pi64, _i, _pvp], _i),
+    "mpsb_mps_batch": ([_vp, C.POINTER(_i)], _i),
+    "mpsb_mps_set_site_copy": ([_vp, _i, _i, _pd], _i),
+    "mpsb_mps_get_site_copy": ([_vp, _i, _i, _pd], _i),
+    "mpsb_mps_view": ([_vp, _i, _pvp], _i),
+    "mpsb_mps_select": ([_vp, _pvp, _i, C.POINTER(_i)], _i),
+    "mpsb_normalize_lo_batch": ([_vp, _vp, _pd], _i),
     "mpsb_mpo_create": ([_vp, _i, _i, _pi64, _pvp], _i),
     "mpsb_mpo_destroy": ([_vp], _i),
     "mpsb_mpo_set_site": ([_vp, _i, _pd], _i),

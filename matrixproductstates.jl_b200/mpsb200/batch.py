@@ -1,0 +1,162 @@
+"""Batched quantum trajectories: many independent trajectories of one chain in one engine.
+
+The reference runs one trajectory per process (examples/spin_model_quantum_trajectory_rk4.jl:
+104-209, one seed per run).  Here trajectories whose bond-dim cap is the same share a bucket:
+the bucket's states live in batch handles (all copies of one MPS shape back to back), and every
+step of the example loop is issued once for the whole bucket --
+
+  * the coherent RK4 step (RK4stp_apply_H_half!) of every copy, one captured CUDA graph whose
+    GEMM, MPO-apply and cluster-QR launches each cover all copies;
+  * the two waveguide-jump compressions compress_var_apply_H!(A_r / A_l, ..., jumpright /
+    jumpleft, 1) of every copy (the reference computes them only on a jump step; computing them
+    for all copies changes nothing for the copies that do not jump and keeps the launches
+    batched);
+  * normalize_lo! of A_coh, A_r and A_l for every copy, one read-back of the norms;
+  * the host decision of each trajectory with its own r1 / r2 stream (the example's branch
+    logic), then one per-copy select A <- A_coh / A_r / A_l; local decays (gam_eg > 0) act on a
+    view of the copy.
+
+Buckets run on their own contexts (streams), so the buckets' kernels overlap on the device.
+Within a bucket every kernel computes each copy exactly as it computes a bucket of one (batched
+calls never split a GEMM's K), so a trajectory's records and state do not depend on which
+other trajectories share its bucket.
+"""
+import numpy as np
+
+from . import core as K
+from . import models as Mo
+
+
+def dims_rule(na, dmax, d):
+    dims = [dmax] * (na + 1)
+    dims[0] = dims[na] = 1
+    for n in range(1, na):
+        dims[n] = min(dims[n - 1] * d, dims[n])
+        dims[na - n] = min(dims[na + 1 - n] * d, dims[na - n])
+    return dims
+
+
+class TrajectoryBucket:
+    """All trajectories of one bond-dim cap `chi`: the example's buffers as batch handles."""
+
+    def __init__(self, p, chi, dt, r1, r2, device=0, ctx=None):
+        self.p, self.chi, self.dt = p, int(chi), dt
+        self.r1, self.r2 = np.atleast_2d(r1), np.atleast_2d(r2)      # [copy, step]
+        self.B = self.r1.shape[0]
+        self.ctx = ctx or K.Context(device)
+        self.own_ctx = ctx is None
+        na = p.na
+        dims = dims_rule(na, self.chi, 2)
+        self.dims = dims
+        B, c = self.B, self.ctx
+        self.A = K.MPS(dims, 2, c, batch=B)
+        state = np.zeros(2, dtype=np.complex128)
+        state[0] = 1.0
+        for k in range(na):   # mpsgroundstate (src/constructors.jl:67-76) in every copy
+            site = np.zeros((dims[k], 2, dims[k + 1]), dtype=np.complex128)
+            site[0, :, 0] = state
+            for b in range(B):
+                self.A.set_site_copy(b, k, site)
+        self.A_coh, self.A_r, self.A_l, self.A1, self.A2, self.A3 = (K.MPS(dims, 2, c, batch=B) for _ in range(6))
+        self.envop = K.build_env(dims, dims, [4] * (na + 1), c, batch=B)
+        self.envop_jump = K.build_env(dims, dims, [2] * (na + 1), c, batch=B)
+        self.env1, self.env2, self.env3 = (K.build_env(dims, dims, None, c, batch=B) for _ in range(3))
+        self.H = [K.MPO.from_sites(Mo.sm_hamiltonian(p, 1, dt / 2, 0.0), c),
+                  K.MPO.from_sites(Mo.sm_hamiltonian(p, 0, 1, dt / 2), c),
+                  K.MPO.from_sites(Mo.sm_hamiltonian(p, 1, dt / 2, dt), c)]
+        jr_, jl_ = Mo.jump_mpos(p, 0.0)
+        self.jumpright = K.MPO.from_sites(jr_, c)
+        self.jumpleft = K.MPO.from_sites(jl_, c)
+        self.p_coh = [[] for _ in range(B)]
+        self.jumps = [[] for _ in range(B)]
+        self.i = 0
+
+    def issue(self):
+        """Enqueue step i's coherent step and jump compressions for every copy (no wait)."""
+        K.RK4stp_apply_H_half_(self.dt, self.H, self.A_coh, self.A, self.A1, self.A2, self.A3,
+                               self.env1, self.env2, self.env3, self.envop)
+        K.compress_var_apply_H_(self.A_r, self.envop_jump, self.A, self.A, self.jumpright, 1)
+        K.compress_var_apply_H_(self.A_l, self.envop_jump, self.A, self.A, self.jumpleft, 1)
+
+    def finish(self):
+        """Norms, per-trajectory decisions of step i, and the state update A <- chosen copy."""
+        i, p, dt, na = self.i, self.p, self.dt, self.p.na
+        p_coh = K.normalize_lo_batch(self.A_coh)
+        p_r = K.normalize_lo_batch(self.A_r)
+        p_l = K.normalize_lo_batch(self.A_l)
+        which = np.full(self.B, -1, dtype=np.int64)
+        local = []
+        for b in range(self.B):
+            self.p_coh[b].append(p_coh[b])
+            if self.r1[b, i] < p_coh[b]:
+                which[b] = 0
+                continue
+            p_acc = np.zeros(na + 3)
+            if p.gam_eg != 0:
+                epop = K.measure_local(self.A.view(b), Mo.E_E)
+                for j in range(na):
+                    p_acc[j + 1] = p_acc[j] + dt * p.gam_eg * epop[j]
+            p_acc[na + 1] = p_acc[na] + dt * p_r[b]
+            p_acc[na + 2] = p_acc[na + 1] + dt * p_l[b]
+            p_sum = p_acc[-1]
+            p_acc = p_acc / p_acc[-1]
+            r = self.r2[b, i]
+            if r < p_acc[na]:
+                for j in range(na):
+                    if r < p_acc[j + 1]:
+                        local.append((b, j))
+                        self.jumps[b].append((i, "local", j + 1, p_coh[b], p_sum))
+                        break
+            elif r < p_acc[na + 1]:
+                which[b] = 1
+                self.jumps[b].append((i, "right", 0, p_coh[b], p_sum))
+            else:
+                which[b] = 2
+                self.jumps[b].append((i, "left", 0, p_coh[b], p_sum))
+        self.A.select([self.A_coh, self.A_r, self.A_l], which)
+        for b, j in local:
+            v = self.A.view(b)
+            K.apply_site_operator_(v, j + 1, Mo.SM)
+            K.leftorthonormalizationQR_(v)
+        self.i += 1
+
+    def close(self):
+        for name in ("A", "A_coh", "A_r", "A_l", "A1", "A2", "A3", "envop", "envop_jump", "env1", "env2", "env3",
+                     "H", "jumpright", "jumpleft"):
+            setattr(self, name, None)
+        if self.own_ctx:
+            self.ctx.close()
+
+
+class TrajectoryBatch:
+    """Trajectories of one chain with per-trajectory bond caps `chis` and uniform streams
+    r1[k], r2[k]; grouped into buckets of equal cap."""
+
+    def __init__(self, p, chis, dt, r1, r2, device=0):
+        self.p, self.dt = p, dt
+        self.chis = [int(c) for c in chis]
+        r1, r2 = np.asarray(r1), np.asarray(r2)
+        self.members = {}
+        for k, c in enumerate(self.chis):
+            self.members.setdefault(c, []).append(k)
+        self.buckets = {c: TrajectoryBucket(p, c, dt, r1[m], r2[m], device) for c, m in sorted(self.members.items())}
+
+    def step(self):
+        for bk in self.buckets.values():
+            bk.issue()
+        for bk in self.buckets.values():
+            bk.finish()
+
+    def records(self, k):
+        """(p_coh, jumps, final sites) of trajectory k."""
+        c = self.chis[k]
+        b = self.members[c].index(k)
+        bk = self.buckets[c]
+        return np.array(bk.p_coh[b]), list(bk.jumps[b]), bk.A.sites_copy(b)
+
+    def site_updates_per_step(self):
+        return self.p.na * len(self.chis)
+
+    def close(self):
+        for bk in self.buckets.values():
+            bk.close()

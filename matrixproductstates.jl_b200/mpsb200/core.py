@@ -92,16 +92,54 @@ def default_context():
 
 
 class MPS:
-    """Device MPS (``Vector{Array{T,3}}``) with fixed bond dims."""
+    """Device MPS (``Vector{Array{T,3}}``) with fixed bond dims.  With ``batch`` (an int) the
+    handle holds that many copies of the shape (a batch handle of the batched engine); site
+    access without ``copy`` addresses copy 0."""
 
-    def __init__(self, dims, d, ctx=None):
+    def __init__(self, dims, d, ctx=None, batch=None):
         self.ctx = ctx or default_context()
         self.dims = [int(x) for x in dims]
         self.na = len(self.dims) - 1
         self.d = int(d)
+        self.batch = 1 if batch is None else int(batch)
+        self.batched = batch is not None
+        self.parent = None
         h = C.c_void_p()
-        _lib.call("mpsb_mps_create", self.ctx.h, self.na, self.d, _i64(self.dims), C.byref(h))
+        if batch is None:
+            _lib.call("mpsb_mps_create", self.ctx.h, self.na, self.d, _i64(self.dims), C.byref(h))
+        else:
+            _lib.call("mpsb_mps_create_batch", self.ctx.h, self.na, self.d, _i64(self.dims), self.batch, C.byref(h))
         self.h = h
+
+    def view(self, copy):
+        """A handle on one copy of a batch handle (shares its memory)."""
+        v = MPS.__new__(MPS)
+        v.ctx, v.dims, v.na, v.d, v.batch, v.batched, v.parent = self.ctx, self.dims, self.na, self.d, 1, False, self
+        h = C.c_void_p()
+        _lib.call("mpsb_mps_view", self.h, int(copy), C.byref(h))
+        v.h = h
+        return v
+
+    def set_site_copy(self, copy, k, a):
+        if tuple(a.shape) != self.shape(k):
+            raise _lib.DimensionMismatch(-2, "set_site", "site %d has shape %s, expected %s" % (k, a.shape, self.shape(k)))
+        buf = _f64(a)
+        _lib.call("mpsb_mps_set_site_copy", self.h, int(copy), k + 1, _dptr(buf))
+
+    def site_copy(self, copy, k):
+        n = int(np.prod(self.shape(k)))
+        buf = np.empty(2 * n, dtype=np.float64)
+        _lib.call("mpsb_mps_get_site_copy", self.h, int(copy), k + 1, _dptr(buf))
+        return buf.view(CT).reshape(self.shape(k), order="F")
+
+    def sites_copy(self, copy):
+        return [self.site_copy(copy, k) for k in range(self.na)]
+
+    def select(self, sources, which):
+        """copy b <- sources[which[b]] copy b (which[b] < 0 keeps copy b)."""
+        arr = (C.c_void_p * len(sources))(*[s.h.value for s in sources])
+        w = (C.c_int * self.batch)(*[int(x) for x in which])
+        _lib.call("mpsb_mps_select", self.h, arr, len(sources), w)
 
     def __del__(self):
         try:
@@ -154,7 +192,7 @@ class MPS:
         return self
 
     def clone(self):
-        return MPS(self.dims, self.d, self.ctx).copy_from(self)
+        return MPS(self.dims, self.d, self.ctx, self.batch if self.batched else None).copy_from(self)
 
 
 class MPO:
@@ -208,15 +246,20 @@ class MPO:
 class Env:
     """``build_env`` buffers (src/constructors.jl:347-375): N+1 entries, ones at both ends."""
 
-    def __init__(self, dims1, dims2, mpo_dims=None, ctx=None):
+    def __init__(self, dims1, dims2, mpo_dims=None, ctx=None, batch=None):
         self.ctx = ctx or default_context()
         self.na = len(dims1) - 1
         self.three = mpo_dims is not None
         self.dims1, self.dims2 = list(dims1), list(dims2)
         self.w = list(mpo_dims) if mpo_dims is not None else [1] * (self.na + 1)
+        self.batch = 1 if batch is None else int(batch)
         h = C.c_void_p()
-        _lib.call("mpsb_env_create", self.ctx.h, self.na, _i64(dims1), _i64(dims2),
-                  _i64(self.w) if self.three else None, C.byref(h))
+        if batch is None:
+            _lib.call("mpsb_env_create", self.ctx.h, self.na, _i64(dims1), _i64(dims2),
+                      _i64(self.w) if self.three else None, C.byref(h))
+        else:
+            _lib.call("mpsb_env_create_batch", self.ctx.h, self.na, _i64(dims1), _i64(dims2),
+                      _i64(self.w) if self.three else None, self.batch, C.byref(h))
         self.h = h
 
     def __del__(self):
@@ -245,8 +288,8 @@ class Env:
         _lib.call("mpsb_env_set", self.h, e + 1, _dptr(buf))
 
 
-def build_env(dims1, dims2, mpo_dims=None, ctx=None):
-    return Env(dims1, dims2, mpo_dims, ctx)
+def build_env(dims1, dims2, mpo_dims=None, ctx=None, batch=None):
+    return Env(dims1, dims2, mpo_dims, ctx, batch)
 
 
 # ------------------------------------------------------------------ constructors
@@ -650,6 +693,13 @@ def _scalar(name, *args):
 def normalize_lo_(mps):
     """src/orthonormalisation.jl:97-103."""
     return _scalar("mpsb_normalize_lo", mps.ctx.h, mps.h)
+
+
+def normalize_lo_batch(mps):
+    """normalize_lo! of every copy of a batch handle; returns the norms^2 before scaling."""
+    out = np.zeros(mps.batch, dtype=np.float64)
+    _lib.call("mpsb_normalize_lo_batch", mps.ctx.h, mps.h, _dptr(out))
+    return out
 
 
 def norm_lo(mps):

@@ -1,0 +1,62 @@
+"""Batched trajectories (mpsb200.batch): many trajectories per bond-dim bucket, every kernel over
+all copies of a bucket at once.
+
+* a trajectory's p_coh record, jump record and final state are bitwise the same in a bucket of
+  one and in a bucket shared with others (and with other buckets running beside it);
+* against the oracle's example loop (oracle/drivers.run_trajectory) with the same uniforms:
+  identical jump records (forced jump steps exercise both waveguide jumps) and p_coh within
+  1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _uniforms(seed, nsteps, forced=()):
+    g = np.random.default_rng(seed)
+    r1, r2 = g.random(nsteps), g.random(nsteps)
+    for i in forced:
+        r1[i] = 1.0 - 1e-12   # above any p_coh < 1: a jump step
+    return r1, r2
+
+
+def _run(p, chis, dt, nsteps, seeds, forced):
+    from mpsb200 import batch as BT
+    r = [_uniforms(s, nsteps, forced) for s in seeds]
+    tb = BT.TrajectoryBatch(p, chis, dt, [x[0] for x in r], [x[1] for x in r])
+    try:
+        for _ in range(nsteps):
+            tb.step()
+        return [tb.records(k) for k in range(len(chis))], r
+    finally:
+        tb.close()
+
+
+def test_batched_equals_alone_bitwise():
+    from mpsb200 import models as GM
+    p = GM.WaveguideChain(10, omega=0.5)
+    chis, seeds, forced = [8, 16, 8, 16, 8], [0, 1, 2, 3, 4], (3, 7)
+    mixed, _ = _run(p, chis, 0.01, 12, seeds, forced)
+    for k, (c, s) in enumerate(zip(chis, seeds)):
+        alone, _ = _run(p, [c], 0.01, 12, [s], forced)
+        pc, jm, st = mixed[k]
+        pa, ja, sa = alone[0]
+        assert np.array_equal(pc, pa) and jm == ja
+        assert all(np.array_equal(x, y) for x, y in zip(st, sa))
+
+
+def test_batched_matches_oracle_jump_records():
+    from mpsb200 import models as GM
+    from oracle import drivers as ODR
+    from oracle import models as OM
+    na, dt, n = 10, 0.01, 12
+    chis, seeds, forced = [8, 8, 16], [5, 6, 7], (2, 5, 9)
+    got, unif = _run(GM.WaveguideChain(na, omega=0.5), chis, dt, n, seeds, forced)
+    for k, c in enumerate(chis):
+        r1, r2 = unif[k]
+        rec = ODR.run_trajectory(OM.SpinChain(na, omega=0.5), c, dt, n, r1, r2, measure_int=n)
+        pc, jm, _ = got[k]
+        assert [(j[0], j[1], j[2]) for j in jm] == [(j[0], j[1], j[2]) for j in rec["jumps"]]
+        assert len(jm) == len(forced)
+        assert np.abs(pc - rec["p_coh"]).max() <= 1e-10
