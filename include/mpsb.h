@@ -81,6 +81,12 @@ int mpsb_ctx_set_precision(mpsb_ctx* ctx, int slices, int min_tiles);
  * counted. */
 int mpsb_ctx_set_profiling(mpsb_ctx* ctx, int enable);
 int mpsb_ctx_profile_read(mpsb_ctx* ctx, double* ms, int64_t* launches);
+/* Failure-detection self-test (no reference counterpart): one device thread waits `seconds`
+ * (0 < seconds <= 10) on a barrier that nothing arrives on, with the bounded wait every pipeline
+ * wait of this library uses; the wait runs out, the kernel sets the context's error word and
+ * returns, and this call returns MPSB_ERR_CUDA with a "timed out" message.  The error word is
+ * cleared by that report, and the context stays usable. */
+int mpsb_wait_selftest(mpsb_ctx* ctx, double seconds);
 /* Kernel launches issued by this context since creation (for accounting). */
 int mpsb_ctx_launch_count(mpsb_ctx* ctx, int64_t* out);
 

@@ -43,7 +43,7 @@ static int sync(mpsb_ctx* ctx) {
     cudaMemsetAsync(ctx->err(), 0, sizeof(int), ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     set_last_message("a device-side wait timed out (%s); results of this stream are invalid",
-                     (*hw & 2) ? "sliced GEMM pipeline" : "QR cluster exchange");
+                     (*hw & 4) ? "wait self-test" : (*hw & 2) ? "sliced GEMM pipeline" : "QR cluster exchange");
     return MPSB_ERR_CUDA;
   }
   return MPSB_OK;
@@ -229,6 +229,13 @@ int mpsb_ctx_profile_read(mpsb_ctx* ctx, double* ms, int64_t* launches) {
   *launches = (int64_t)ctx->prof_events.size();
   ctx->prof_events.clear();
   return MPSB_OK;
+}
+
+int mpsb_wait_selftest(mpsb_ctx* ctx, double seconds) {
+  MPSB_TRY(bind(ctx));
+  count_launch(&ctx->ws);
+  MPSB_TRY(wait_probe_launch(seconds, ctx->err(), ctx->stream));
+  return sync(ctx);
 }
 
 int mpsb_ctx_set_precision(mpsb_ctx* ctx, int slices, int min_tiles) {

@@ -79,12 +79,12 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 // wait for the phase of the given parity, bounded in wall-clock time; false when it ran out
-__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long limit_ns = WAIT_NS) {
   if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   for (unsigned i = 1;; ++i) {
     if (mbar_test(bar, parity)) return true;
-    if ((i & 255) == 0 && global_ns() - t0 > WAIT_NS) return false;
+    if ((i & 255) == 0 && global_ns() - t0 > limit_ns) return false;
     __nanosleep(32);
   }
 }
@@ -417,6 +417,19 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   }
 }
 
+// Self-test of the bounded wait: one thread waits on an mbarrier that nothing ever arrives on;
+// the wait runs out after limit_ns and the kernel reports it in the error word (bit 2) and
+// returns.  Nothing else is in flight, so the context stays usable.
+__global__ void wait_probe_kernel(unsigned long long limit_ns, int* err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0, limit_ns)) atomicOr(err, 4);
+}
+
 // ---------------------------------------------------------------- host side
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
@@ -496,6 +509,13 @@ int smem_of(int S) {
 inline int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
+
+int wait_probe_launch(double seconds, int* err, cudaStream_t s) {
+  if (!(seconds > 0.0) || seconds > 10.0 || !err) return MPSB_ERR_INVALID_ARG;
+  wait_probe_kernel<<<1, 32, 0, s>>>((unsigned long long)(seconds * 1e9), err);
+  MPSB_CUDA_TRY(cudaGetLastError());
+  return MPSB_OK;
+}
 
 bool ozgemm_supported(const Gemm& g, int slices) {
   if (slices < OZ_MIN_SLICES || slices > OZ_MAX_SLICES) return false;

@@ -156,3 +156,21 @@ def test_split_rk4_random_start_fidelity():
     scale = max(max(abs(x[0]), np.abs(x[1]).max(), np.abs(x[2]).max()) for x in o64)
     assert _obs_err(o6, o64) <= 1e-8 * scale
     assert 1 - fidelity(s6, s64) <= 1e-10
+
+
+def test_bounded_wait_runs_out_and_the_context_recovers(gpu_ctx):
+    """Failure detection without a fault: a device wait on a barrier nothing arrives on gives up
+    after 50 ms, the call reports the timeout through the error word, and the same context then
+    computes a sliced GEMM correctly."""
+    import time
+
+    from mpsb200 import _lib
+    t0 = time.perf_counter()
+    with pytest.raises(_lib.MpsbError) as e:
+        _lib.call("mpsb_wait_selftest", gpu_ctx.h, 0.05)
+    assert e.value.status == -3 and "timed out" in str(e.value)
+    assert time.perf_counter() - t0 < 5.0
+    rng = np.random.default_rng(12)
+    A, B = crand(rng, 96, 64), crand(rng, 64, 40)
+    got = zgemm(gpu_ctx, A, B, slices=6)
+    assert np.abs(got - A @ B).max() <= 4 * 2.0 ** -42 * 128 * np.abs(A).max() * np.abs(B).max()
