@@ -50,13 +50,13 @@ class TrajectoryBucket:
         self.dims = dims
         B, c = self.B, self.ctx
         self.A = K.MPS(dims, 2, c, batch=B)
-        state = np.zeros(2, dtype=np.complex128)
-        state[0] = 1.0
-        for k in range(na):   # mpsgroundstate (src/constructors.jl:67-76) in every copy
-            site = np.zeros((dims[k], 2, dims[k + 1]), dtype=np.complex128)
-            site[0, :, 0] = state
+        # mpsgroundstate (src/constructors.jl:67-76): the padded product state left-orthogonalised
+        # by the QR sweep (its zero-weight columns are the Householder ones), in every copy
+        start, _ = K.mpsgroundstate(na, self.chi, 2, c)
+        for k, site in enumerate(start.sites()):
             for b in range(B):
                 self.A.set_site_copy(b, k, site)
+        del start
         self.A_coh, self.A_r, self.A_l, self.A1, self.A2, self.A3 = (K.MPS(dims, 2, c, batch=B) for _ in range(6))
         self.envop = K.build_env(dims, dims, [4] * (na + 1), c, batch=B)
         self.envop_jump = K.build_env(dims, dims, [2] * (na + 1), c, batch=B)
