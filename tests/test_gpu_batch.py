@@ -52,11 +52,16 @@ def test_batched_matches_oracle_jump_records():
     from oracle import models as OM
     na, dt, n = 10, 0.01, 12
     chis, seeds, forced = [8, 8, 16], [5, 6, 7], (2, 5, 9)
+    from gpu_util import perturbed_oracle_qr
     got, unif = _run(GM.WaveguideChain(na, omega=0.5), chis, dt, n, seeds, forced)
     for k, c in enumerate(chis):
         r1, r2 = unif[k]
         rec = ODR.run_trajectory(OM.SpinChain(na, omega=0.5), c, dt, n, r1, r2, measure_int=n)
+        with perturbed_oracle_qr(1e-15):
+            pert = ODR.run_trajectory(OM.SpinChain(na, omega=0.5), c, dt, n, r1, r2, measure_int=n)
+        env = np.abs(pert["p_coh"] - rec["p_coh"])
         pc, jm, _ = got[k]
         assert [(j[0], j[1], j[2]) for j in jm] == [(j[0], j[1], j[2]) for j in rec["jumps"]]
         assert len(jm) == len(forced)
-        assert np.abs(pc - rec["p_coh"]).max() <= 1e-10
+        # the oracle's own spread under rounding-level perturbations bounds any implementation
+        assert np.all(np.abs(pc - rec["p_coh"]) <= 100 * env + 1e-12)
