@@ -40,6 +40,10 @@ WORKLOADS = {
                       slices=6, pairs=((0, 1), (29, 30), (9, 49)), golden="rho_n60_chi512.npz"),
     "density": dict(na=40, d=4, chi=128, chi0=0, seed=0, w=8, dt=0.005, gam_eg=0.1, omega=0.5, gam_phi=0.1,
                     slices=0, pairs=((0, 1), (9, 10), (19, 20), (4, 34)), golden="rho_n40_chi128.npz"),
+    # independent trajectories of the driven waveguide chain (d=2, w=4), per-trajectory bond caps
+    # log-uniform over 8..256 on a 16-value grid, every trajectory its own seed
+    "batch": dict(na=64, d=2, chi=256, w=4, dt=0.01, omega=0.5, ntraj=256, chi_seed=3, slices=6,
+                  grid=[int(round(8 * 32 ** (j / 15.0))) for j in range(16)]),
 }
 METRIC = "MPS site-updates/s (RK4 step)"
 UNIT = "site-updates/s"
@@ -473,7 +477,63 @@ def cpu_rate(W, nsamples):
     return nsamples * (fl / mean_site) / tot, tot / nsamples, fl, mean_site
 
 
+def batch_chis(W):
+    """Per-trajectory bond caps: u_k ~ U[0,1) (seeded), chi_k = the grid value nearest to 8*32^u_k
+    on the log scale."""
+    import numpy as np
+    u = np.random.default_rng(W["chi_seed"]).random(W["ntraj"])
+    g = np.log(np.array(W["grid"], dtype=float))
+    return [W["grid"][int(np.argmin(np.abs(g - np.log(8 * 32 ** x))))] for x in u]
+
+
+def batch_flops(W, chis):
+    """Algorithmic flops of one step of every trajectory: the RK4 step of step_flops plus the
+    two jump compressions (one R->L and one L->R sweep with the w=2 jump MPO, compress_var_apply_H!
+    with maxsweeps = 1 after its environment initialisation)."""
+    tot = 0.0
+    for c in set(chis):
+        n = chis.count(c)
+        dims = dims_rule(W["na"], c, W["d"])
+        wv = [1] + [W["w"]] * (W["na"] - 1) + [1]
+        f = sum(step_flops(dims, wv, W["d"]).values())
+        wj = [1] + [2] * (W["na"] - 1) + [1]
+        fj = step_flops_jump(dims, wj, W["d"])
+        tot += n * (f + 2 * fj)
+    return tot
+
+
+def step_flops_jump(dims, w, d):
+    """flops of compress_var_apply_H!(A0, envop, A, A, H, 1): left env init, one R->L and one
+    L->R sweep (prod_AOR/AOL, prod_LR, QR, env update per site)."""
+    na = len(dims) - 1
+    f = 0.0
+    for k in range(na):
+        Dl, Dr, wl, wr = dims[k], dims[k + 1], w[k], w[k + 1]
+        aol = 8.0 * (wl * Dl) * (d * Dr) * Dl + 8.0 * Dl * Dr * (wl * d) * (d * wr)
+        aor = 8.0 * (Dl * d) * (wr * Dr) * Dr + 8.0 * Dl * Dr * (d * wr) * (wl * d)
+        if k < na - 1:
+            f += aol + 8.0 * (Dr * wr) * Dr * (Dl * d)                                  # init
+            f += aol + 8.0 * (Dl * d) * Dr * (Dr * wr) + 16.0 * ((d * Dl) * Dr * Dr - Dr ** 3 / 3.0) \
+                + 8.0 * (Dr * wr) * Dr * (Dl * d)                                       # L->R sweep
+        else:
+            f += aol + 8.0 * (Dl * d) * Dr * (Dr * wr)
+        if k > 0:
+            f += aor + 8.0 * Dl * (d * Dr) * (Dl * wl) + 16.0 * ((d * Dr) * Dl * Dl - Dl ** 3 / 3.0) \
+                + 8.0 * (Dl * wl) * Dl * (d * Dr)                                       # R->L sweep
+    return f
+
+
 def config_dict(args, W):
+    if args.workload == "batch":
+        return {"workload": "%d independent quantum trajectories of the driven waveguide chain N=%d, d=2, w=4, "
+                            "dt=%g, bond caps log-uniform 8..256 (16-value grid), all-down start; one step = the "
+                            "example loop's step of every trajectory (RK4 step, both jump compressions, norms, "
+                            "jump decisions); contractions int8-sliced x%d on tcgen05 (the larger ones), QR / "
+                            "norms FP64" % (W["ntraj"], W["na"], W["dt"], W["slices"]),
+                "name": "batch", "trajectories": W["ntraj"], "sites": W["na"], "d": 2, "w": 4, "dt": W["dt"],
+                "chi_grid": W["grid"], "slices": W["slices"],
+                "parallelism": "replicas x%d; trajectories grouped in per-chi buckets, one stream each" % args.gpus,
+                "l2": "working set per step > 126 MB L2 (no flush needed)"}
     return {"workload": "density-matrix RK4 step, waveguide spin chain N=%d, d=%d, chi=%d, w=%d (6 + 2 zero "
                         "channels), dt=%g, %s start%s" % (
                             W["na"], W["d"], W["chi"], W["w"], W["dt"],
@@ -491,6 +551,21 @@ def run_reference(args, rank):
     if rank != 0:
         return None
     W = WORKLOADS[args.workload]
+    if args.workload == "batch":
+        chis = batch_chis(W)
+        model, cores = cpu_info()
+        cb = None
+        vals = []
+        for _ in range(max(1, args.steps)):
+            cb = batch_cpu_baseline(W, chis)
+            vals.append(cb["value"])
+        value = sum(vals) / len(vals)
+        cb["value"] = value
+        return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": 0, "ms_per_step": 1e3 * W["na"] * W["ntraj"] / value,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+                "data": "synthetic (all-down trajectories)", "config": config_dict(args, W), "cpu_baseline": cb,
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     model, cores = cpu_info()
     for _ in range(args.warmup):
         oracle_site_sample(W)
@@ -546,7 +621,7 @@ def time_sliced_gemm(ctx, torch, stream, W):
     ctx.set_profiling(True)
     for _ in range(reps):
         _lib.call("mpsb_op_zgemm", *args)
-    ms, n = ctx.profile_read()
+    ms, n, _ = ctx.profile_read()
     ctx.set_profiling(False)
     del A, B, Cm
     int8_ops = 2.0 * (S * (S + 1) // 2) * M * (2 * N) * (2 * Kd)
@@ -753,6 +828,157 @@ def run_ours(args, rank, world, local_rank, dist):
     return line
 
 
+def _uniforms(seed, n):
+    import numpy as np
+    g = np.random.default_rng(seed)
+    return g.random(n), g.random(n)
+
+
+def run_batch(args, rank, world, local_rank, dist):
+    """The batching workload: every trajectory's step through the bucketed batch engine, split
+    precision (the headline), beside the same engine in FP64 and the plain FP64 path that runs
+    one trajectory at a time (the drop-in, as the reference runs one trajectory per process)."""
+    import numpy as np
+    import torch
+
+    import mpsb200 as K
+    from mpsb200 import batch as BT
+    from mpsb200 import drivers as GDR
+    from mpsb200 import models as GM
+
+    torch.cuda.set_device(local_rank)
+    W = WORKLOADS["batch"]
+    chis = batch_chis(W)
+    n = args.warmup + args.steps
+    unif = [_uniforms(1000003 * rank + k, n) for k in range(W["ntraj"])]
+    r1 = np.array([u[0] for u in unif])
+    r2 = np.array([u[1] for u in unif])
+    p = GM.WaveguideChain(W["na"], omega=W["omega"])
+    flops_step = batch_flops(W, chis)
+
+    def timed(slices, sample_clocks=False, profile=False):
+        tb = BT.TrajectoryBatch(p, chis, W["dt"], r1, r2, device=local_rank, slices=slices)
+        for _ in range(args.warmup):
+            tb.step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        sampler = ClockSampler(local_rank) if sample_clocks else None
+        if sampler:
+            sampler.start()
+        l0 = sum(bk.ctx.launches for bk in tb.buckets.values())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        for _ in range(args.steps):
+            tb.step()
+        torch.cuda.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        clocks = sampler.stop() if sampler else None
+        launches = sum(bk.ctx.launches for bk in tb.buckets.values()) - l0
+        secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
+        prof = None
+        if profile:   # one more step with the tensor-core kernel bracketed by events
+            for bk in tb.buckets.values():
+                bk.ctx.set_graphs(False)
+                bk.ctx.set_profiling(True)
+                bk.ctx.profile_read()
+            tb.step()
+            ms = ops = cnt = 0.0
+            for bk in tb.buckets.values():
+                a, c_, o = bk.ctx.profile_read()
+                ms, cnt, ops = ms + a, cnt + c_, ops + o
+                bk.ctx.set_profiling(False)
+            prof = (ms, cnt, ops)
+        recs = [tb.records(k)[:2] for k in range(W["ntraj"])]
+        tb.close()
+        return secs, wall, launches, clocks, recs, prof
+
+    secs, wall, launches, clocks, recs, prof = timed(W["slices"], sample_clocks=True, profile=True)
+    value = job_rate(world, W["na"] * W["ntraj"], args.steps, secs)
+    secs64, _, _, _, recs64, _ = timed(0)
+    value64 = job_rate(world, W["na"] * W["ntraj"], args.steps, secs64)
+    dp = max(float(np.abs(np.asarray(a[0]) - np.asarray(b[0])).max()) for a, b in zip(recs, recs64))
+    same_jumps = sum(1 for a, b in zip(recs, recs64) if [j[:3] for j in a[1]] == [j[:3] for j in b[1]])
+    njumps = sum(len(a[1]) for a in recs)
+
+    # the plain FP64 path, one trajectory at a time: per distinct cap, one trajectory's step time
+    plain_t = {}
+    for c in sorted(set(chis)):
+        ctx = K.Context(local_rank)
+        b = GDR.TrajectoryBuffers(p, c, W["dt"], ctx)
+        rec = {"p_coh": [], "jumps": []}
+        for i in range(n):
+            if i == 1:
+                ctx.sync()
+                t0 = time.perf_counter()
+            pc = b.coherent_step()
+            GDR.trajectory_decision(b, i, pc, r1[0], r2[0], rec)
+        ctx.sync()
+        plain_t[c] = (time.perf_counter() - t0) / (n - 1)
+        del b
+        ctx.close()
+    plain_secs = sum(plain_t[c] for c in chis)   # one step of every trajectory, one after the other
+    value_plain = job_rate(world, W["na"] * W["ntraj"], 1, plain_secs)
+
+    peak, src = load_peaks()
+    ms, cnt, ops = prof
+    ach = ops / (ms * 1e-3) / 1e12 if ms > 0 else None
+    roofline = {"bound": "tensor", "pipe": "int8 (tcgen05 kind::i8)", "kernel": "ozgemm_kernel<%d>" % W["slices"],
+                "achieved": ach, "peak": peak, "unit": "TOP/s", "frac": ach / peak if ach else None,
+                "peak_source": src, "traffic": None,
+                "per_launch": "all %d launches of one step of the workload (every bucket, CUDA events around each "
+                              "launch): %.3e int8 ops in %.2f ms" % (cnt, ops, ms)}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "complex128 operands, int8 slices x%d on the tensor pipe for the larger contractions, FP64 "
+                 "QR/norms/jump probabilities" % W["slices"],
+        "data": "synthetic (all-down trajectories, seeded uniforms, waveguide H)",
+        "config": config_dict(args, W), "clocks": clocks, "gpu_launches": int(launches),
+        "step_tflops": flops_step * args.steps / secs * world / 1e12,
+        "fp64_batched": {"value": value64, "ms_per_step": 1e3 * secs64 / args.steps, "split_vs_fp64_batched": value / value64},
+        "fp64_plain_one_at_a_time": {"value": value_plain, "s_per_step_all_trajectories": plain_secs,
+                                     "per_chi_s_per_step": plain_t,
+                                     "split_batched_vs_plain": value / value_plain},
+        "roofline": roofline,
+        "e2e": {"value": job_rate(world, W["na"] * W["ntraj"], args.steps, max_over_ranks(wall, dist)),
+                "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 3 * 8 * W["ntraj"],
+                "note": "the step is host-driven through the public API: every bucket's norms of A_coh, A_r, "
+                        "A_l come back each step for the jump decisions"},
+        "check": {"p_coh_max_abs_err_split_vs_fp64": dp, "trajectories_same_jump_record": same_jumps,
+                  "trajectories": W["ntraj"], "jumps": njumps},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = batch_cpu_baseline(W, chis)
+    return line
+
+
+def batch_cpu_baseline(W, chis, grid=None):
+    """CPU oracle on the batching workload: one coherent step (no jump) of one trajectory per
+    distinct cap of the sample, timed; the mix's rate = trajectories x sites / sum of their times."""
+    import numpy as np
+
+    from oracle import drivers as ODR
+    from oracle import models as OM
+    model, cores = cpu_info()
+    t = {}
+    for c in sorted(set(chis) if grid is None else grid):
+        p = OM.SpinChain(W["na"], omega=W["omega"])
+        t0 = time.perf_counter()
+        ODR.run_trajectory(p, c, W["dt"], 1, np.zeros(1), np.zeros(1), measure_int=10)
+        t[c] = time.perf_counter() - t0
+    tot = sum(t[c] for c in chis)
+    value = W["na"] * len(chis) / tot
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "one RK4 step (no jump) of one trajectory per distinct bond cap (%d caps) on the CPU oracle "
+                      "(NumPy/OpenBLAS, %s, %d threads), weighted by the caps' counts; %.1f s for the sample"
+                      % (len(t), model, cores, sum(t.values()))}
+
+
 def main():
     if "--op" in sys.argv:
         i = sys.argv.index("--op")
@@ -789,7 +1015,10 @@ def main():
         __graft_entry__.build()   # no-op when libmpsb200.so is current
     if dist:
         dist.barrier()
-    line = run_ours(args, rank, world, local_rank, dist)
+    if args.workload == "batch":
+        line = run_batch(args, rank, world, local_rank, dist)
+    else:
+        line = run_ours(args, rank, world, local_rank, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -76,11 +76,11 @@ int mpsb_ctx_set_pipeline(mpsb_ctx* ctx, int enable);
 int mpsb_ctx_set_precision(mpsb_ctx* ctx, int slices, int min_tiles);
 /* Device-time accounting of the sliced path's tensor-core GEMM kernel (no reference
  * counterpart): while enabled, every eager launch of that kernel is bracketed by CUDA events;
- * mpsb_ctx_profile_read waits for the context, returns the summed milliseconds and the number
- * of launches since the last read, and clears them.  Launches inside captured graphs are not
- * counted. */
+ * mpsb_ctx_profile_read waits for the context, returns the summed milliseconds, the number of
+ * launches and their int8 operations since the last read, and clears them.  Launches inside
+ * captured graphs are not counted. */
 int mpsb_ctx_set_profiling(mpsb_ctx* ctx, int enable);
-int mpsb_ctx_profile_read(mpsb_ctx* ctx, double* ms, int64_t* launches);
+int mpsb_ctx_profile_read(mpsb_ctx* ctx, double* ms, int64_t* launches, double* int8_ops /* or NULL */);
 /* Failure-detection self-test (no reference counterpart): one device thread waits `seconds`
  * (0 < seconds <= 10) on a barrier that nothing arrives on, with the bounded wait every pipeline
  * wait of this library uses; the wait runs out, the kernel sets the context's error word and

@@ -164,8 +164,8 @@ int mpsb_ctx_destroy(mpsb_ctx* ctx) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   cudaStreamSynchronize(ctx->side);
   for (auto& p : ctx->prof_events) {
-    cudaEventDestroy(p.first);
-    cudaEventDestroy(p.second);
+    cudaEventDestroy(p.start);
+    cudaEventDestroy(p.stop);
   }
   ws_free(ctx->ws);
   ws_free(ctx->ws_side);
@@ -212,20 +212,22 @@ int mpsb_ctx_set_profiling(mpsb_ctx* ctx, int enable) {
   return MPSB_OK;
 }
 
-int mpsb_ctx_profile_read(mpsb_ctx* ctx, double* ms, int64_t* launches) {
+int mpsb_ctx_profile_read(mpsb_ctx* ctx, double* ms, int64_t* launches, double* ops) {
   MPSB_TRY(bind(ctx));
   if (!ms || !launches) return MPSB_ERR_INVALID_ARG;
   MPSB_TRY(sync(ctx));
   MPSB_CUDA_TRY(cudaStreamSynchronize(ctx->side));
-  double tot = 0.0;
+  double tot = 0.0, nops = 0.0;
   for (auto& p : ctx->prof_events) {
     float t = 0.f;
-    MPSB_CUDA_TRY(cudaEventElapsedTime(&t, p.first, p.second));
+    MPSB_CUDA_TRY(cudaEventElapsedTime(&t, p.start, p.stop));
     tot += t;
-    cudaEventDestroy(p.first);
-    cudaEventDestroy(p.second);
+    nops += p.ops;
+    cudaEventDestroy(p.start);
+    cudaEventDestroy(p.stop);
   }
   *ms = tot;
+  if (ops) *ops = nops;
   *launches = (int64_t)ctx->prof_events.size();
   ctx->prof_events.clear();
   return MPSB_OK;

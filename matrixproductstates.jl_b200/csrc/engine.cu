@@ -49,7 +49,6 @@ struct BatchScope {
         prev_split(ctx->split_on) {
     c->batch = B;
     c->ws.no_splitk = c->ws_side.no_splitk = batched;
-    if (batched) c->split_on = false;
   }
   ~BatchScope() {
     c->batch = prev;
@@ -79,7 +78,10 @@ static int call_batch(std::initializer_list<const mpsb_mps*> mps, std::initializ
   return MPSB_OK;
 }
 
+// Whether a sweep GEMM takes the sliced path: by its output tiles (a plain call), or -- in a
+// batched call, where the decision must not depend on the batch size -- by its own work alone.
 static bool split_worth(const mpsb_ctx* ctx, const Gemm& g) {
+  if (ctx->ws.no_splitk) return 8.0 * g.M * g.N * g.K >= (double)(1 << 24) && g.K >= 16;
   const int64_t tiles = ((int64_t)(g.M + 127) / 128) * ((2 * (int64_t)g.N + 63) / 64);
   return tiles >= ctx->split_min_tiles && g.K >= 16;
 }

@@ -57,7 +57,7 @@ struct mpsb_ctx {
     int seen = 0;
   };
   std::map<std::vector<int64_t>, GraphEntry> graphs_cache;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;   // see mpsb_ctx_set_profiling
+  std::vector<mpsb::Workspace::TimedLaunch> prof_events;   // see mpsb_ctx_set_profiling
 };
 
 struct mpsb_mps {

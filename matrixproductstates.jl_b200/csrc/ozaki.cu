@@ -149,13 +149,16 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
 // the pair of rows (n,re) = [re, -im], (n,im) = [im, re] of B'^T; otherwise a row is [re, im].
 struct SliceView {
   const cd* X; int R, K; int64_t x_r, x_k; bool conj;
+  int64_t x_bat;   // element offset between the problems of a batch (blockIdx.z)
 };
 
 // biased IEEE exponent of max(|re|, |im|) (0 for zero / subnormal), max-reduced per row into
 // rexp (zeroed before)
-__global__ void oz_rowexp_kernel(SliceView v, int* __restrict__ rexp) {
+__global__ void oz_rowexp_kernel(SliceView v, int* __restrict__ rexp0, int64_t rexp_bat) {
   __shared__ int tile_e[32][33];
   const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  v.X += (int64_t)blockIdx.z * v.x_bat;
+  int* rexp = rexp0 + (int64_t)blockIdx.z * rexp_bat;
   const int tid = threadIdx.x;
   const bool rc = (v.x_r == 1);   // rows contiguous: lanes run along r
   for (int i = 0; i < 4; ++i) {
@@ -201,10 +204,13 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
 // Digits of a 32-row x 32-complex tile: out[t][row][k'] (K' = 2K padded to Kp, rows padded to
 // the tile grid with zeros, so every byte the GEMM reads is written).
 template <int S, bool BMODE>
-__global__ void oz_split_kernel(SliceView v, const int* __restrict__ rexp, int8_t* __restrict__ out, int64_t rows_out,
-                                int Kp) {
+__global__ void oz_split_kernel(SliceView v, const int* __restrict__ rexp0, int64_t rexp_bat, int8_t* __restrict__ out0,
+                                int64_t rows_out, int Kp) {
   __shared__ cd tile[32][33];
   const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  v.X += (int64_t)blockIdx.z * v.x_bat;
+  const int* rexp = rexp0 + (int64_t)blockIdx.z * rexp_bat;
+  int8_t* out = out0 + (int64_t)blockIdx.z * S * rows_out * Kp;
   const int tid = threadIdx.x;
   const bool rc = (v.x_r == 1);
   for (int i = 0; i < 4; ++i) {
@@ -255,9 +261,11 @@ struct OzParams {
   int kstages;           // K' / OZ_BK
   const int* ea;         // biased exponents per row of A (Mpad)
   const int* eb;         // biased exponents per complex column of B (NBpad / 2)
-  cd* C; int64_t c_m, c_n;
+  cd* C; int64_t c_m, c_n, c_bat;
   cd alpha, beta;
   int* err;              // device error word (bit 1: a wait in this kernel ran out)
+  // problem blockIdx.y of a batch: its slices start at row blockIdx.y * S * Mpad (* NBpad) of
+  // the tensor maps, its exponents at blockIdx.y * Mpad (* NBpad / 2)
 };
 
 template <int S>
@@ -278,6 +286,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   const int tiles_m = P.Mpad / OZ_BM;
   const int m_tile = blockIdx.x % tiles_m, n_tile = blockIdx.x / tiles_m;
   const int m0 = m_tile * OZ_BM, n0 = n_tile * OZ_BN;   // n0 in real columns of C'
+  const int prob = blockIdx.y;
+  const int yA = prob * S * P.Mpad, yB = prob * S * P.NBpad;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; ++s) {
@@ -314,10 +324,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         unsigned char* st = smem + s * SB;
         mbar_expect_tx(full + s, SB);
 #pragma unroll
-        for (int i = 0; i < S; ++i) tma_load_2d(st + i * A_TILE, &tmA, full + s, kb * OZ_BK, i * P.Mpad + m0);
+        for (int i = 0; i < S; ++i) tma_load_2d(st + i * A_TILE, &tmA, full + s, kb * OZ_BK, yA + i * P.Mpad + m0);
 #pragma unroll
         for (int j = 0; j < S; ++j)
-          tma_load_2d(st + S * A_TILE + j * B_TILE, &tmB, full + s, kb * OZ_BK, j * P.NBpad + n0);
+          tma_load_2d(st + S * A_TILE + j * B_TILE, &tmB, full + s, kb * OZ_BK, yB + j * P.NBpad + n0);
         issued = kb + 1;
       }
       if (*abort_flag) {
@@ -369,7 +379,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     const int row = 32 * (warp - 4) + lane;
     const int m = m0 + row;
     const uint32_t tbase = tmem + ((uint32_t)(32 * (warp - 4)) << 16);
-    const int Ea = P.ea[m];
+    const int Ea = P.ea[(int64_t)prob * P.Mpad + m];
+    const int* eb = P.eb + (int64_t)prob * (P.NBpad / 2);
+    cd* Cp = P.C + (int64_t)prob * P.c_bat;
     const bool use_beta = (P.beta.x != 0.0) || (P.beta.y != 0.0);
     const bool good = ok && !*abort_flag;
 #pragma unroll 1
@@ -392,14 +404,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         for (int c = 0; c < 16; ++c) {
           const int n = nbase + c;
           if (n < P.N) {
-            const int Eb = P.eb[n];
+            const int Eb = eb[n];
             double re = 0.0, im = 0.0;
             if (Ea > 0 && Eb > 0) {
               const int e = (Ea - 1022) + (Eb - 1022);
               re = ldexp(acc[2 * c], e);
               im = ldexp(acc[2 * c + 1], e);
             }
-            cd* cp = P.C + (int64_t)m * P.c_m + (int64_t)n * P.c_n;
+            cd* cp = Cp + (int64_t)m * P.c_m + (int64_t)n * P.c_n;
             cd val = cmul(P.alpha, cmk(re, im));
             if (use_beta) val = cadd(val, cmul(P.beta, *cp));
             *cp = val;
@@ -466,7 +478,7 @@ int make_map(CUtensorMap* map, const int8_t* base, int64_t kp, int64_t rows, int
 }
 
 typedef void (*OzKernel)(CUtensorMap, CUtensorMap, OzParams);
-typedef void (*SplitKernel)(SliceView, const int*, int8_t*, int64_t, int);
+typedef void (*SplitKernel)(SliceView, const int*, int64_t, int8_t*, int64_t, int);
 
 template <int S>
 struct OzTable {
@@ -519,7 +531,7 @@ int wait_probe_launch(double seconds, int* err, cudaStream_t s) {
 
 bool ozgemm_supported(const Gemm& g, int slices) {
   if (slices < OZ_MIN_SLICES || slices > OZ_MAX_SLICES) return false;
-  if (g.batch != 1 || g.M <= 0 || g.N <= 0 || g.K <= 0) return false;
+  if (g.batch < 1 || g.batch > 65535 || g.M <= 0 || g.N <= 0 || g.K <= 0) return false;
   // exact int32 accumulation: S * 127^2 * 2K < 2^31
   return (int64_t)slices * 127 * 127 * 2 * (int64_t)g.K < (int64_t(1) << 31);
 }
@@ -527,7 +539,7 @@ bool ozgemm_supported(const Gemm& g, int slices) {
 size_t ozgemm_scratch_bytes(const Gemm& g, int slices) {
   const int64_t Mpad = round_up(g.M, OZ_BM), NBpad = round_up(2 * (int64_t)g.N, OZ_BN);
   const int64_t Kp = round_up(2 * (int64_t)g.K, OZ_KP_ALIGN);
-  return (size_t)slices * (Mpad + NBpad) * Kp + (size_t)(Mpad + NBpad / 2) * sizeof(int) + 1024;
+  return (size_t)g.batch * ((size_t)slices * (Mpad + NBpad) * Kp + (size_t)(Mpad + NBpad / 2) * sizeof(int)) + 1024;
 }
 
 int ozgemm_launch(const Gemm& g, int slices, void* scratch, size_t scratch_bytes, int* err, Workspace* ws,
@@ -538,56 +550,65 @@ int ozgemm_launch(const Gemm& g, int slices, void* scratch, size_t scratch_bytes
   const int S = slices;
   const int64_t Mpad = round_up(g.M, OZ_BM), NBpad = round_up(2 * (int64_t)g.N, OZ_BN);
   const int64_t Kp = round_up(2 * (int64_t)g.K, OZ_KP_ALIGN);
-  if (Mpad * S >= (int64_t(1) << 31) || NBpad * S >= (int64_t(1) << 31) || Kp >= (int64_t(1) << 31))
+  const int64_t B = g.batch;
+  if (B * Mpad * S >= (int64_t(1) << 31) || B * NBpad * S >= (int64_t(1) << 31) || Kp >= (int64_t(1) << 31))
     return MPSB_ERR_UNSUPPORTED;
+  // scratch: the A slices of every problem [B][S][Mpad][Kp], then the B slices [B][S][NBpad][Kp],
+  // then the row exponents [B][Mpad] and the column exponents [B][NBpad / 2]
   int8_t* sa = static_cast<int8_t*>(scratch);
-  int8_t* sb = sa + (size_t)S * Mpad * Kp;
-  int* ea = reinterpret_cast<int*>(sb + (size_t)S * NBpad * Kp);
-  int* eb = ea + Mpad;
-  MPSB_CUDA_TRY(cudaMemsetAsync(ea, 0, (size_t)(Mpad + NBpad / 2) * sizeof(int), s));
+  int8_t* sb = sa + (size_t)B * S * Mpad * Kp;
+  int* ea = reinterpret_cast<int*>(sb + (size_t)B * S * NBpad * Kp);
+  int* eb = ea + B * Mpad;
+  MPSB_CUDA_TRY(cudaMemsetAsync(ea, 0, (size_t)B * (Mpad + NBpad / 2) * sizeof(int), s));
 
   // A' rows = rows m of op(A): element (m, k) at A[m a_m + k a_k]
-  SliceView va{g.A, g.M, g.K, g.a_m, g.a_k, g.conjA};
+  SliceView va{g.A, g.M, g.K, g.a_m, g.a_k, g.conjA, g.a_b};
   // B'^T rows come from columns n of op(B): element (n, k) at B[n b_n + k b_k]
-  SliceView vb{g.B, g.N, g.K, g.b_n, g.b_k, g.conjB};
+  SliceView vb{g.B, g.N, g.K, g.b_n, g.b_k, g.conjB, g.b_b};
   const int kc = (int)(Kp / 2);   // complex k extent covered by the slice grid
+  const unsigned bz = (unsigned)B;
   count_launch(ws);
-  oz_rowexp_kernel<<<dim3((unsigned)((g.M + 31) / 32), (unsigned)((g.K + 31) / 32)), 256, 0, s>>>(va, ea);
+  oz_rowexp_kernel<<<dim3((unsigned)((g.M + 31) / 32), (unsigned)((g.K + 31) / 32), bz), 256, 0, s>>>(va, ea, Mpad);
   MPSB_CUDA_TRY(cudaGetLastError());
   count_launch(ws);
-  oz_rowexp_kernel<<<dim3((unsigned)((g.N + 31) / 32), (unsigned)((g.K + 31) / 32)), 256, 0, s>>>(vb, eb);
+  oz_rowexp_kernel<<<dim3((unsigned)((g.N + 31) / 32), (unsigned)((g.K + 31) / 32), bz), 256, 0, s>>>(vb, eb,
+                                                                                                      NBpad / 2);
   MPSB_CUDA_TRY(cudaGetLastError());
   count_launch(ws);
-  pick_split(S, false)<<<dim3((unsigned)(Mpad / 32), (unsigned)(kc / 32)), 256, 0, s>>>(va, ea, sa, Mpad, (int)Kp);
+  pick_split(S, false)<<<dim3((unsigned)(Mpad / 32), (unsigned)(kc / 32), bz), 256, 0, s>>>(va, ea, Mpad, sa, Mpad,
+                                                                                          (int)Kp);
   MPSB_CUDA_TRY(cudaGetLastError());
   count_launch(ws);
-  pick_split(S, true)<<<dim3((unsigned)(NBpad / 64), (unsigned)(kc / 32)), 256, 0, s>>>(vb, eb, sb, NBpad, (int)Kp);
+  pick_split(S, true)<<<dim3((unsigned)(NBpad / 64), (unsigned)(kc / 32), bz), 256, 0, s>>>(vb, eb, NBpad / 2, sb,
+                                                                                          NBpad, (int)Kp);
   MPSB_CUDA_TRY(cudaGetLastError());
 
   CUtensorMap ta, tb;
-  MPSB_TRY(make_map(&ta, sa, Kp, S * Mpad, OZ_BM));
-  MPSB_TRY(make_map(&tb, sb, Kp, S * NBpad, OZ_BN));
+  MPSB_TRY(make_map(&ta, sa, Kp, B * S * Mpad, OZ_BM));
+  MPSB_TRY(make_map(&tb, sb, Kp, B * S * NBpad, OZ_BN));
   OzParams P;
   P.M = g.M; P.N = g.N; P.Mpad = (int)Mpad; P.NBpad = (int)NBpad; P.kstages = (int)(Kp / OZ_BK);
   P.ea = ea; P.eb = eb;
-  P.C = g.C; P.c_m = g.c_m; P.c_n = g.c_n; P.alpha = g.alpha; P.beta = g.beta;
+  P.C = g.C; P.c_m = g.c_m; P.c_n = g.c_n; P.c_bat = g.c_b; P.alpha = g.alpha; P.beta = g.beta;
   P.err = err;
   OzKernel fn = pick_gemm(S);
   MPSB_TRY(ensure_kernel_attrs((const void*)fn, smem_of(S)));
   const int64_t tiles = (Mpad / OZ_BM) * (NBpad / OZ_BN);
   if (tiles >= (int64_t(1) << 31)) return MPSB_ERR_UNSUPPORTED;
   count_launch(ws);
-  std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+  Workspace::TimedLaunch ev{nullptr, nullptr, 0.0};
   const bool timed = ws && ws->prof && !ws->capturing;
   if (timed) {
-    MPSB_CUDA_TRY(cudaEventCreate(&ev.first));
-    MPSB_CUDA_TRY(cudaEventCreate(&ev.second));
-    MPSB_CUDA_TRY(cudaEventRecord(ev.first, s));
+    MPSB_CUDA_TRY(cudaEventCreate(&ev.start));
+    MPSB_CUDA_TRY(cudaEventCreate(&ev.stop));
+    MPSB_CUDA_TRY(cudaEventRecord(ev.start, s));
+    // S(S+1)/2 slice products of the real (M x 2K) x (2K x 2N) GEMM per problem, 2 ops per MAC
+    ev.ops = 2.0 * (S * (S + 1) / 2) * (double)g.M * (2.0 * g.N) * (2.0 * g.K) * (double)B;
   }
-  fn<<<(unsigned)tiles, OZ_THREADS, smem_of(S), s>>>(ta, tb, P);
+  fn<<<dim3((unsigned)tiles, bz), OZ_THREADS, smem_of(S), s>>>(ta, tb, P);
   MPSB_CUDA_TRY(cudaGetLastError());
   if (timed) {
-    MPSB_CUDA_TRY(cudaEventRecord(ev.second, s));
+    MPSB_CUDA_TRY(cudaEventRecord(ev.stop, s));
     ws->prof->push_back(ev);
   }
   return MPSB_OK;

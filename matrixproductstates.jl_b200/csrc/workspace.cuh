@@ -26,7 +26,11 @@ struct Workspace {
   int64_t launches = 0;   // kernel launches issued (eager) or recorded (capture)
   // when set (and not capturing), the sliced GEMM brackets its tensor-core kernel with a pair of
   // CUDA events appended here, so its device time can be read apart from the slicing kernels
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* prof = nullptr;
+  struct TimedLaunch {
+    cudaEvent_t start, stop;
+    double ops;   // int8 operations of the launch
+  };
+  std::vector<TimedLaunch>* prof = nullptr;
 };
 
 inline void count_launch(Workspace* ws) {

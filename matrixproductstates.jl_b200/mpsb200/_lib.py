@@ -39,7 +39,7 @@ SIGNATURES = {
     "mpsb_ctx_set_precision": ([_vp, _i, _i], _i),
     "mpsb_wait_selftest": ([_vp, _d], _i),
     "mpsb_ctx_set_profiling": ([_vp, _i], _i),
-    "mpsb_ctx_profile_read": ([_vp, _pd, _pi64], _i),
+    "mpsb_ctx_profile_read": ([_vp, _pd, _pi64, _pd], _i),
     "mpsb_ctx_launch_count": ([_vp, _pi64], _i),
     "mpsb_mps_create": ([_vp, _i, _i, _pi64, _pvp], _i),
     "mpsb_mps_destroy": ([_vp], _i),

@@ -39,12 +39,13 @@ def dims_rule(na, dmax, d):
 class TrajectoryBucket:
     """All trajectories of one bond-dim cap `chi`: the example's buffers as batch handles."""
 
-    def __init__(self, p, chi, dt, r1, r2, device=0, ctx=None):
+    def __init__(self, p, chi, dt, r1, r2, device=0, ctx=None, slices=0):
         self.p, self.chi, self.dt = p, int(chi), dt
         self.r1, self.r2 = np.atleast_2d(r1), np.atleast_2d(r2)      # [copy, step]
         self.B = self.r1.shape[0]
         self.ctx = ctx or K.Context(device)
         self.own_ctx = ctx is None
+        self.ctx.set_precision(slices)
         na = p.na
         dims = dims_rule(na, self.chi, 2)
         self.dims = dims
@@ -130,16 +131,18 @@ class TrajectoryBucket:
 
 class TrajectoryBatch:
     """Trajectories of one chain with per-trajectory bond caps `chis` and uniform streams
-    r1[k], r2[k]; grouped into buckets of equal cap."""
+    r1[k], r2[k]; grouped into buckets of equal cap; `slices` > 0 puts the sweeps' larger
+    contractions on the int8-sliced tensor-core path (see Context.set_precision)."""
 
-    def __init__(self, p, chis, dt, r1, r2, device=0):
+    def __init__(self, p, chis, dt, r1, r2, device=0, slices=0):
         self.p, self.dt = p, dt
         self.chis = [int(c) for c in chis]
         r1, r2 = np.asarray(r1), np.asarray(r2)
         self.members = {}
         for k, c in enumerate(self.chis):
             self.members.setdefault(c, []).append(k)
-        self.buckets = {c: TrajectoryBucket(p, c, dt, r1[m], r2[m], device) for c, m in sorted(self.members.items())}
+        self.buckets = {c: TrajectoryBucket(p, c, dt, r1[m], r2[m], device, slices=slices)
+                        for c, m in sorted(self.members.items())}
 
     def step(self):
         for bk in self.buckets.values():

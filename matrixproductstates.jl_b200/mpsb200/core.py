@@ -61,10 +61,10 @@ class Context:
         _lib.call("mpsb_ctx_set_profiling", self.h, 1 if enable else 0)
 
     def profile_read(self):
-        """(milliseconds, launches) of the tensor-core GEMM kernel since the last read."""
-        ms, n = C.c_double(), C.c_int64()
-        _lib.call("mpsb_ctx_profile_read", self.h, C.byref(ms), C.byref(n))
-        return ms.value, n.value
+        """(milliseconds, launches, int8 ops) of the tensor-core GEMM kernel since the last read."""
+        ms, n, ops = C.c_double(), C.c_int64(), C.c_double()
+        _lib.call("mpsb_ctx_profile_read", self.h, C.byref(ms), C.byref(n), C.byref(ops))
+        return ms.value, n.value, ops.value
 
     def set_stream(self, stream_ptr):
         _lib.call("mpsb_ctx_set_stream", self.h, C.c_void_p(stream_ptr or 0))

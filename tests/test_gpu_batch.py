@@ -21,10 +21,10 @@ def _uniforms(seed, nsteps, forced=()):
     return r1, r2
 
 
-def _run(p, chis, dt, nsteps, seeds, forced):
+def _run(p, chis, dt, nsteps, seeds, forced, slices=0):
     from mpsb200 import batch as BT
     r = [_uniforms(s, nsteps, forced) for s in seeds]
-    tb = BT.TrajectoryBatch(p, chis, dt, [x[0] for x in r], [x[1] for x in r])
+    tb = BT.TrajectoryBatch(p, chis, dt, [x[0] for x in r], [x[1] for x in r], slices=slices)
     try:
         for _ in range(nsteps):
             tb.step()
@@ -65,3 +65,20 @@ def test_batched_matches_oracle_jump_records():
         assert len(jm) == len(forced)
         # the oracle's own spread under rounding-level perturbations bounds any implementation
         assert np.all(np.abs(pc - rec["p_coh"]) <= 100 * env + 1e-12)
+
+
+def test_batched_split_precision_equals_alone_and_stays_near_fp64():
+    """The sliced tensor-core path inside batched buckets (N=14, bonds up to 128): bitwise the
+    same alone and in a shared bucket, and within 1e-9 of the FP64 batched run on p_coh."""
+    from mpsb200 import models as GM
+    p = GM.WaveguideChain(14, omega=0.5)
+    chis, seeds, forced = [128, 64, 128], [8, 9, 10], (4,)
+    mixed, _ = _run(p, chis, 0.01, 8, seeds, forced, slices=6)
+    fp, _ = _run(p, chis, 0.01, 8, seeds, forced, slices=0)
+    for k, (c, s) in enumerate(zip(chis, seeds)):
+        alone, _ = _run(p, [c], 0.01, 8, [s], forced, slices=6)
+        assert np.array_equal(mixed[k][0], alone[0][0]) and mixed[k][1] == alone[0][1]
+        assert all(np.array_equal(x, y) for x, y in zip(mixed[k][2], alone[0][2]))
+        assert [j[:3] for j in mixed[k][1]] == [j[:3] for j in fp[k][1]]
+        assert np.abs(mixed[k][0] - fp[k][0]).max() <= 1e-9
+        assert any(np.abs(x - y).max() > 0 for x, y in zip(mixed[k][2], fp[k][2]))   # the path is taken
