@@ -849,7 +849,7 @@ def run_batch(args, rank, world, local_rank, dist):
     torch.cuda.set_device(local_rank)
     W = WORKLOADS["batch"]
     chis = batch_chis(W)
-    n = args.warmup + args.steps
+    n = args.warmup + args.steps + 1      # + the profiled step
     unif = [_uniforms(1000003 * rank + k, n) for k in range(W["ntraj"])]
     r1 = np.array([u[0] for u in unif])
     r2 = np.array([u[1] for u in unif])
