@@ -900,8 +900,10 @@ def run_batch(args, rank, world, local_rank, dist):
     value = job_rate(world, W["na"] * W["ntraj"], args.steps, secs)
     secs64, _, _, _, recs64, _ = timed(0)
     value64 = job_rate(world, W["na"] * W["ntraj"], args.steps, secs64)
-    dp = max(float(np.abs(np.asarray(a[0]) - np.asarray(b[0])).max()) for a, b in zip(recs, recs64))
-    same_jumps = sum(1 for a, b in zip(recs, recs64) if [j[:3] for j in a[1]] == [j[:3] for j in b[1]])
+    dp = max(float(np.abs(np.asarray(a[0])[:len(b[0])] - np.asarray(b[0])).max()) for a, b in zip(recs, recs64))
+    nb = args.warmup + args.steps
+    same_jumps = sum(1 for a, b in zip(recs, recs64)
+                     if [j[:3] for j in a[1] if j[0] < nb] == [j[:3] for j in b[1] if j[0] < nb])
     njumps = sum(len(a[1]) for a in recs)
 
     # the plain FP64 path, one trajectory at a time: per distinct cap, one trajectory's step time
