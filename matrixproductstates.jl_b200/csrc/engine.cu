@@ -3,6 +3,7 @@
 // launches of the strided GEMM, MPO-apply and cluster-QR kernels on the context stream.
 #include <algorithm>
 #include <cstring>
+#include <functional>
 
 #include "engine.cuh"
 #include "ozaki.cuh"
@@ -484,6 +485,60 @@ int compress_var_apply_H_left(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, cons
   return compress_sum_var_apply_H(ctx, false, A0, nullptr, envop, Ain, c1, 1, terms, H);
 }
 
+// Run `body` (a fixed sequence of launches on the context's streams) through the context's graph
+// cache: the first call runs eagerly and sizes every scratch buffer, the second captures the
+// launches into a CUDA graph, later calls replay it; a reallocated scratch buffer (generation
+// counter) sends the key back to eager execution.  With graphs off, the body runs eagerly.
+static int run_cached(mpsb_ctx* ctx, const std::vector<int64_t>& key, const std::function<int()>& body) {
+  if (!ctx->graphs) return body();
+  auto& ent = ctx->graphs_cache[key];
+  if (ent.exec && ent.generation == ctx->ws_generation) {
+    ctx->ws.launches += ent.launches;
+    MPSB_CUDA_TRY(cudaGraphLaunch(ent.exec, ctx->stream));
+    return MPSB_OK;
+  }
+  if (ent.exec) {
+    cudaGraphExecDestroy(ent.exec);
+    ent.exec = nullptr;
+    ent.seen = 0;
+  }
+  if (ent.seen == 0) {  // eager first call sizes every scratch buffer
+    ent.seen = 1;
+    return body();
+  }
+  const int64_t gen0 = ctx->ws_generation;
+  const int64_t l0 = ctx->ws.launches + ctx->ws_side.launches;
+  ctx->ws.capturing = ctx->ws_side.capturing = true;
+  MPSB_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int st = body();
+  cudaGraph_t g = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->ws.capturing = ctx->ws_side.capturing = false;
+  if (st != MPSB_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (ce != cudaSuccess) {
+    set_last_error(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+    return MPSB_ERR_CUDA;
+  }
+  cudaGraphExec_t exec = nullptr;
+  ce = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    set_last_error(ce, "cudaGraphInstantiate", __FILE__, __LINE__);
+    return MPSB_ERR_CUDA;
+  }
+  ent.exec = exec;
+  ent.generation = gen0;
+  ent.launches = ctx->ws.launches + ctx->ws_side.launches - l0;
+  MPSB_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
+  return MPSB_OK;
+}
+
+static int compress_var_apply_H_body(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain,
+                                     const mpsb_mps* A, const mpsb_mpo* H, int maxsweeps);
+
 // compress_var_apply_H! (src/compression.jl:217-258): maxsweeps R->L / L->R sweep pairs
 int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain, const mpsb_mps* A,
                          const mpsb_mpo* H, int maxsweeps) {
@@ -494,6 +549,13 @@ int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mps
   bool batched;
   MPSB_TRY(call_batch({A0, Ain, A}, {envop}, &B, &batched));
   BatchScope bscope(ctx, B, batched);
+  std::vector<int64_t> key = {2, ctx->split_slices, ctx->split_min_tiles, B, maxsweeps, A0->serial, envop->serial,
+                              Ain->serial, A->serial, H->serial};
+  return run_cached(ctx, key, [&]() { return compress_var_apply_H_body(ctx, A0, envop, Ain, A, H, maxsweeps); });
+}
+
+static int compress_var_apply_H_body(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mpsb_mps* Ain,
+                                     const mpsb_mps* A, const mpsb_mpo* H, int maxsweeps) {
   const int na = A0->na, d = A0->d;
   for (int k = 0; k <= na; ++k)
     if (envop->d1[k] != A0->dims[k] || envop->d2[k] != A0->dims[k] || envop->w[k] != H->w[k]) return MPSB_ERR_DIMENSION;
@@ -784,56 +846,14 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
   bool batched;
   MPSB_TRY(call_batch({psi0, psi, psi1, psi2, psi3}, {env1, env2, env3, envop}, &B, &batched));
   BatchScope bscope(ctx, B, batched);
-  if (!ctx->graphs)
-    return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
   int64_t dtbits;
   std::memcpy(&dtbits, &dt, sizeof(dt));
-  std::vector<int64_t> key = {ctx->pipeline ? 2 : 1, ctx->split_slices, ctx->split_min_tiles, B, dtbits, H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial,
-                              psi1->serial, psi2->serial, psi3->serial, env1->serial, env2->serial,
-                              env3->serial, envop->serial};
-  auto& ent = ctx->graphs_cache[key];
-  if (ent.exec && ent.generation == ctx->ws_generation) {
-    ctx->ws.launches += ent.launches;
-    MPSB_CUDA_TRY(cudaGraphLaunch(ent.exec, ctx->stream));
-    return MPSB_OK;
-  }
-  if (ent.exec) {
-    cudaGraphExecDestroy(ent.exec);
-    ent.exec = nullptr;
-    ent.seen = 0;
-  }
-  if (ent.seen == 0) {  // eager first call sizes every scratch buffer
-    ent.seen = 1;
+  std::vector<int64_t> key = {1, ctx->pipeline ? 2 : 1, ctx->split_slices, ctx->split_min_tiles, B, dtbits,
+                              H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial, psi1->serial,
+                              psi2->serial, psi3->serial, env1->serial, env2->serial, env3->serial, envop->serial};
+  return run_cached(ctx, key, [&]() {
     return rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
-  }
-  const int64_t gen0 = ctx->ws_generation;
-  const int64_t l0 = ctx->ws.launches + ctx->ws_side.launches;
-  ctx->ws.capturing = ctx->ws_side.capturing = true;
-  MPSB_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  int st = rk4_body(ctx, dt, H1, H2, H3, psi0, psi, psi1, psi2, psi3, env1, env2, env3, envop);
-  cudaGraph_t g = nullptr;
-  cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
-  ctx->ws.capturing = ctx->ws_side.capturing = false;
-  if (st != MPSB_OK) {
-    if (g) cudaGraphDestroy(g);
-    return st;
-  }
-  if (ce != cudaSuccess) {
-    set_last_error(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
-    return MPSB_ERR_CUDA;
-  }
-  cudaGraphExec_t exec = nullptr;
-  ce = cudaGraphInstantiate(&exec, g, 0);
-  cudaGraphDestroy(g);
-  if (ce != cudaSuccess) {
-    set_last_error(ce, "cudaGraphInstantiate", __FILE__, __LINE__);
-    return MPSB_ERR_CUDA;
-  }
-  ent.exec = exec;
-  ent.generation = gen0;
-  ent.launches = ctx->ws.launches + ctx->ws_side.launches - l0;
-  MPSB_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
-  return MPSB_OK;
+  });
 }
 
 }  // namespace mpsb
