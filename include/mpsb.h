@@ -109,8 +109,9 @@ int mpsb_mps_copy(mpsb_mps* dst, const mpsb_mps* src);
  * process, examples/spin_model_quantum_trajectory_rk4.jl:104-107).  A batch handle holds `batch`
  * copies of one MPS shape back to back; every entry point that takes MPS / environment handles
  * accepts batch handles of one common batch size (MPOs are shared by all copies) and runs each
- * kernel over all copies at once.  Calls on batch handles, or on views of one copy, never split a
- * GEMM's K, so a copy computes the same bits in a batch of any size.  Copies are 0-based. */
+ * kernel over all copies at once.  In calls on batch handles, or on views of one copy, every
+ * per-kernel choice (a GEMM's split-K partition, the sliced path) depends on one copy's shape
+ * only, so a copy computes the same bits in a batch of any size.  Copies are 0-based. */
 int mpsb_mps_create_batch(mpsb_ctx* ctx, int na, int d, const int64_t* dims, int batch, mpsb_mps** out);
 int mpsb_env_create_batch(mpsb_ctx* ctx, int na, const int64_t* dims1, const int64_t* dims2,
                           const int64_t* w /* na+1 or NULL */, int batch, mpsb_env** out);

@@ -39,22 +39,22 @@ int ensure_slot(mpsb_ctx* ctx, Slot s, size_t bytes, cd** out) {
 
 // The copies of a batched call: every MPS and environment handle of the call must hold the same
 // number of copies; a handle created as part of a batch (or a view of one copy) puts the call in
-// batched mode (no split-K, no sliced path), so that a copy computes the same bits in a batch of
-// any size.  While alive, kernels of the context run ctx->batch copies.
+// batched mode (split-K and the sliced-path choice decided per problem), so that a copy computes
+// the same bits in a batch of any size.  While alive, kernels of the context run ctx->batch copies.
 struct BatchScope {
   mpsb_ctx* c;
   int prev;
   bool prev_ns, prev_ns_side, prev_split;
   BatchScope(mpsb_ctx* ctx, int B, bool batched)
-      : c(ctx), prev(ctx->batch), prev_ns(ctx->ws.no_splitk), prev_ns_side(ctx->ws_side.no_splitk),
+      : c(ctx), prev(ctx->batch), prev_ns(ctx->ws.per_problem), prev_ns_side(ctx->ws_side.per_problem),
         prev_split(ctx->split_on) {
     c->batch = B;
-    c->ws.no_splitk = c->ws_side.no_splitk = batched;
+    c->ws.per_problem = c->ws_side.per_problem = batched;
   }
   ~BatchScope() {
     c->batch = prev;
-    c->ws.no_splitk = prev_ns;
-    c->ws_side.no_splitk = prev_ns_side;
+    c->ws.per_problem = prev_ns;
+    c->ws_side.per_problem = prev_ns_side;
     c->split_on = prev_split;
   }
 };
@@ -82,7 +82,7 @@ static int call_batch(std::initializer_list<const mpsb_mps*> mps, std::initializ
 // Whether a sweep GEMM takes the sliced path: by its output tiles (a plain call), or -- in a
 // batched call, where the decision must not depend on the batch size -- by its own work alone.
 static bool split_worth(const mpsb_ctx* ctx, const Gemm& g) {
-  if (ctx->ws.no_splitk) return 8.0 * g.M * g.N * g.K >= (double)(1 << 24) && g.K >= 16;
+  if (ctx->ws.per_problem) return 8.0 * g.M * g.N * g.K >= (double)(1 << 24) && g.K >= 16;
   const int64_t tiles = ((int64_t)(g.M + 127) / 128) * ((2 * (int64_t)g.N + 63) / 64);
   return tiles >= ctx->split_min_tiles && g.K >= 16;
 }

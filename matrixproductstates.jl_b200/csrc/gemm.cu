@@ -271,8 +271,9 @@ int gemm_launch(const Gemm& g, Workspace* ws, cudaStream_t s) {
   // without a workspace (ws == nullptr) K is never split, so no scratch is needed
   // splits of at least two K tiles (measured on the RK4 step, 40 sites at chi=128, d=4:
   // 87.4 ms with >= 4 tiles per split from KT >= 8, 82.7 ms with >= 2 from KT >= 4)
-  if (ws && !ws->no_splitk && ctas < target && KT >= 4) {
-    splits = (int)std::min<int64_t>((target + ctas - 1) / ctas, KT / 2);
+  const int64_t basis = (ws && ws->per_problem) ? (int64_t)tiles : ctas;
+  if (ws && basis < target && KT >= 4) {
+    splits = (int)std::min<int64_t>((target + basis - 1) / basis, KT / 2);
     splits = std::max(1, std::min(splits, 32));
   }
   int kt_per = (KT + splits - 1) / splits;

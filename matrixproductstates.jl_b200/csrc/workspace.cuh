@@ -20,9 +20,10 @@ struct Workspace {
   DevBuf oz;              // sliced tensor-core GEMM: int8 slices of both operands, row exponents
   DevBuf named[16];       // per-sweep temporaries (see engine.cu)
   bool capturing = false;
-  // batched calls: the GEMMs never split K, so every copy of a batch computes exactly what the
-  // same problem computes alone (split-K partitions depend on the grid size)
-  bool no_splitk = false;
+  // batched calls: a GEMM's split-K partition is chosen from one problem's shape alone (not
+  // from the batch's grid), so every copy of a batch computes exactly what the same problem
+  // computes in a batch of one
+  bool per_problem = false;
   int64_t launches = 0;   // kernel launches issued (eager) or recorded (capture)
   // when set (and not capturing), the sliced GEMM brackets its tensor-core kernel with a pair of
   // CUDA events appended here, so its device time can be read apart from the slicing kernels

@@ -7,19 +7,20 @@ step of the example loop is issued once for the whole bucket --
 
   * the coherent RK4 step (RK4stp_apply_H_half!) of every copy, one captured CUDA graph whose
     GEMM, MPO-apply and cluster-QR launches each cover all copies;
-  * the two waveguide-jump compressions compress_var_apply_H!(A_r / A_l, ..., jumpright /
-    jumpleft, 1) of every copy (the reference computes them only on a jump step; computing them
-    for all copies changes nothing for the copies that do not jump and keeps the launches
+  * normalize_lo! of A_coh for every copy, one read-back of the norms;
+  * on a step where some copy jumps (r1 >= p_coh), the two waveguide-jump compressions
+    compress_var_apply_H!(A_r / A_l, ..., jumpright / jumpleft, 1) and their normalize_lo! for
+    every copy of the bucket (the reference computes them only on its jump steps; computing them
+    for the bucket's other copies as well changes nothing for those and keeps the launches
     batched);
-  * normalize_lo! of A_coh, A_r and A_l for every copy, one read-back of the norms;
   * the host decision of each trajectory with its own r1 / r2 stream (the example's branch
     logic), then one per-copy select A <- A_coh / A_r / A_l; local decays (gam_eg > 0) act on a
     view of the copy.
 
 Buckets run on their own contexts (streams), so the buckets' kernels overlap on the device.
 Within a bucket every kernel computes each copy exactly as it computes a bucket of one (batched
-calls never split a GEMM's K), so a trajectory's records and state do not depend on which
-other trajectories share its bucket.
+calls choose every kernel's partition from one copy's shape), so a trajectory's records and
+state do not depend on which other trajectories share its bucket.
 """
 import numpy as np
 
@@ -73,18 +74,20 @@ class TrajectoryBucket:
         self.i = 0
 
     def issue(self):
-        """Enqueue step i's coherent step and jump compressions for every copy (no wait)."""
+        """Enqueue step i's coherent step for every copy (no wait)."""
         K.RK4stp_apply_H_half_(self.dt, self.H, self.A_coh, self.A, self.A1, self.A2, self.A3,
                                self.env1, self.env2, self.env3, self.envop)
-        K.compress_var_apply_H_(self.A_r, self.envop_jump, self.A, self.A, self.jumpright, 1)
-        K.compress_var_apply_H_(self.A_l, self.envop_jump, self.A, self.A, self.jumpleft, 1)
 
     def finish(self):
         """Norms, per-trajectory decisions of step i, and the state update A <- chosen copy."""
         i, p, dt, na = self.i, self.p, self.dt, self.p.na
         p_coh = K.normalize_lo_batch(self.A_coh)
-        p_r = K.normalize_lo_batch(self.A_r)
-        p_l = K.normalize_lo_batch(self.A_l)
+        p_r = p_l = None
+        if np.any(self.r1[:, i] >= p_coh):   # a jump step for some copy
+            K.compress_var_apply_H_(self.A_r, self.envop_jump, self.A, self.A, self.jumpright, 1)
+            p_r = K.normalize_lo_batch(self.A_r)
+            K.compress_var_apply_H_(self.A_l, self.envop_jump, self.A, self.A, self.jumpleft, 1)
+            p_l = K.normalize_lo_batch(self.A_l)
         which = np.full(self.B, -1, dtype=np.int64)
         local = []
         for b in range(self.B):
