@@ -73,6 +73,12 @@ class TrajectoryBucket:
         self.jumps = [[] for _ in range(B)]
         self.i = 0
 
+    def refresh_h(self, host_sites):
+        """Upload the three generator MPOs of this step from host site arrays (the example loop's
+        update_h!, examples/spin_model_quantum_trajectory_rk4.jl:115-118)."""
+        for mpo, sites in zip(self.H, host_sites):
+            mpo.set_sites(sites)
+
     def issue(self):
         """Enqueue step i's coherent step for every copy (no wait)."""
         K.RK4stp_apply_H_half_(self.dt, self.H, self.A_coh, self.A, self.A1, self.A2, self.A3,
@@ -147,8 +153,18 @@ class TrajectoryBatch:
         self.buckets = {c: TrajectoryBucket(p, c, dt, r1[m], r2[m], device, slices=slices)
                         for c, m in sorted(self.members.items())}
 
-    def step(self):
+    def generator_sites(self, t):
+        """Host site arrays of the step's three generator MPOs at time t (H[1..3] of the example)."""
+        p, dt = self.p, self.dt
+        return [Mo.sm_hamiltonian(p, 1, dt / 2, t), Mo.sm_hamiltonian(p, 0, 1, t + dt / 2),
+                Mo.sm_hamiltonian(p, 1, dt / 2, t + dt)]
+
+    def step(self, host_h=None):
+        """One step of every trajectory; with host_h (generator_sites of the step's time) the
+        generators are uploaded first, as the example loop refreshes them every step."""
         for bk in self.buckets.values():
+            if host_h is not None:
+                bk.refresh_h(host_h)
             bk.issue()
         for bk in self.buckets.values():
             bk.finish()
