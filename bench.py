@@ -1,25 +1,26 @@
 #!/usr/bin/env python
 """Benchmark of the RK4 MPS/MPO time step (RK4stp_apply_H_half!, src/timeevolution.jl:178-196).
 
-Workload (default, --workload precision): vectorised density matrix of the driven waveguide spin
-chain, N=60 sites, d=4, bond dim chi=512, Lindbladian MPO of width w=8 (the exact w=6 MPO plus
-two zero channels), dt=0.005, started from a random chi=64 MPS (complex Gaussian, seed 60,
-left-orthogonal, unit norm) zero-padded to chi=512; one step = one in-place 4-stage RK4 step
-(10-argument form) of the whole chain.  Metric: site-updates/s = sites x steps / time, with the
-step's contractions on the int8-sliced tensor-core path (6 slices) and its QR / norms in FP64;
-the plain FP64 path is timed on the same state beside it, and the observables of the two are
-compared after every warm-up step (the error of the split path against FP64) and against the
-oracle's golden values of the first steps.  --workload density: the plain-FP64 configuration
-(N=40, chi=128, all-down start).
+Workload (default, --workload batch): 256 independent quantum trajectories of the driven waveguide
+chain (N=64 two-level sites, d=2, exact MPO w=4, dt=0.01, all-down start), bond caps log-uniform
+over 8..256 on a 16-value grid, each trajectory its own seeded uniform stream; one step = one
+step of the trajectory example loop for every trajectory (examples/spin_model_quantum_trajectory_
+rk4.jl:104-209: the RK4 step, the norm, the jump decision, the jump compressions on jump steps).
+Measured: the batched engine with the larger contractions on the int8-sliced tensor-core path
+(the headline), the same engine in FP64, and the plain FP64 path running the trajectories one
+at a time (the drop-in); the p_coh records of split and FP64 are compared step by step.
+--workload precision: one density matrix N=60, d=4, chi=512, w=8 from a random chi=64 start,
+split path beside FP64, per-step observable errors, the FP64 sensitivity envelope and a
+physical-start accuracy check.  --workload density: the plain-FP64 density matrix N=40, chi=128.
+Metric: site-updates/s = trajectories x sites x steps / time.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload precision|density]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload batch|precision|density]
     python bench.py --op qr|gemm-mix|zgemm|rk4 ...        per-operation timing (see run_op)
 
-Our arm: device-resident state, CUDA-event timing of K steps on the library stream (max over
-ranks); each rank evolves its own independent density matrix (replicas, weak scaling).
-Reference arm (--impl reference): the CPU oracle (NumPy/OpenBLAS restatement of the
-reference's Julia code, which cannot run here) on the host cores, rank 0 only, on a bounded
-sample of the workload.
+Our arm: device-resident state, CUDA-event timing of K steps (max over ranks); each rank runs its
+own independent replica of the workload (weak scaling).  Reference arm (--impl reference): the
+CPU oracle (NumPy/OpenBLAS restatement of the reference's Julia code, which cannot run here) on
+the host cores, rank 0 only, on a bounded sample of the workload.
 """
 import argparse
 import json
