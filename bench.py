@@ -963,6 +963,8 @@ def run_batch(args, rank, world, local_rank, dist):
         "check": {"p_coh_max_abs_err_split_vs_fp64": dp, "trajectories_same_jump_record": same_jumps,
                   "trajectories": W["ntraj"], "jumps": njumps},
     }
+    if world == 1 and not args.no_serve:
+        line["serving"] = run_serving()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = batch_cpu_baseline(W, chis)
     return line
