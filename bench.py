@@ -226,12 +226,14 @@ def run_op(argv):
         bench.py --op qr M N                     mpsb_op_qr (leftorth!/rightorth!, src/orthonormalisation.jl:164-234)
         bench.py --op gemm-mix [--chi --d --w]   prod_LR (3,4) / (4,3), update_re!, update_le! of one interior site
         bench.py --op zgemm M N K [--slices S]   mpsb_op_zgemm, FP64 (S=0) or int8-sliced tensor-core path
+        bench.py --op batch [--slices S]          steps of the batching workload, each inside an NVTX range
+                                                 "batch_step"
         bench.py --op rk4 [N] [--chi --w --slices S --random CHI0]
                                                  in-place RK4 steps of the density-matrix workload, each timed
                                                  step inside an NVTX range "rk4_step"
     """
     ap = argparse.ArgumentParser(prog="bench.py --op")
-    ap.add_argument("op", choices=["qr", "gemm-mix", "zgemm", "rk4"])
+    ap.add_argument("op", choices=["qr", "gemm-mix", "zgemm", "rk4", "batch"])
     ap.add_argument("dims", nargs="*", type=int)
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
@@ -256,7 +258,29 @@ def run_op(argv):
     ctx.set_stream(stream.cuda_stream)
     g = torch.Generator(device="cuda").manual_seed(1234)
     out = {"op": a.op}
-    if a.op == "qr":
+    if a.op == "batch":
+        import numpy as np
+        from mpsb200 import batch as BT, models as GM
+        W = WORKLOADS["batch"]
+        chis = batch_chis(W)
+        n = a.warmup + a.reps
+        u = [_uniforms(k, n) for k in range(len(chis))]
+        tb = BT.TrajectoryBatch(GM.WaveguideChain(W["na"], omega=W["omega"]), chis, W["dt"],
+                                np.array([x[0] for x in u]), np.array([x[1] for x in u]), slices=a.slices)
+        for _ in range(a.warmup):
+            tb.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(a.reps):
+            torch.cuda.nvtx.range_push("batch_step")
+            tb.step()
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
+        ms = (time.perf_counter() - t0) * 1e3 / a.reps
+        tb.close()
+        out.update({"trajectories": len(chis), "slices": a.slices, "ms_per_step": ms,
+                    "site_updates_per_s": W["na"] * len(chis) / ms * 1e3})
+    elif a.op == "qr":
         m, n = a.dims[:2] if len(a.dims) >= 2 else (512, 128)
         X = torch.randn(m * n, dtype=torch.complex128, device="cuda", generator=g)
         Q = torch.empty_like(X)
