@@ -157,6 +157,35 @@ function ground_state_search!(ctx::Ctx, At::DMPS, H::DMPO, maxsweeps::Integer, c
 end
 
 # normalize_lo!(mps)   src/orthonormalisation.jl:97-103
+# Contraction precision of the sweeps (no reference counterpart): 0 = FP64, 3..7 = int8 slices on
+# the tensor cores for GEMMs of at least `min_tiles` output tiles.
+set_precision!(ctx::Ctx, slices::Integer, min_tiles::Integer = 64) =
+    check(ccall((:mpsb_ctx_set_precision, LIB), Cint, (Ptr{Cvoid}, Cint, Cint), ctx.h, slices, min_tiles),
+          :mpsb_ctx_set_precision)
+
+# B copies of the sites A (a batch handle: every engine call on it runs all copies per kernel)
+function DMPS(ctx::Ctx, A::Vector{<:Array{ComplexF64,3}}, B::Integer)
+    dims = Int64[1; [size(a, 3) for a in A]]
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:mpsb_mps_create_batch, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Int64}, Cint, Ptr{Ptr{Cvoid}}),
+                ctx.h, length(A), size(A[1], 2), dims, B, r), :mpsb_mps_create_batch)
+    m = DMPS(r[], dims, size(A[1], 2))
+    for b in 0:B-1, (j, a) in enumerate(A)
+        check(ccall((:mpsb_mps_set_site_copy, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{ComplexF64}), m.h, b, j, a),
+              :mpsb_mps_set_site_copy)
+    end
+    finalizer(x -> ccall((:mpsb_mps_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), m)
+    return m
+end
+
+# normalize_lo! of every copy of a batch handle: the norms^2 before scaling
+function normalize_lo_batch!(ctx::Ctx, A::DMPS, B::Integer)
+    no = zeros(Float64, B)
+    check(ccall((:mpsb_normalize_lo_batch, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}), ctx.h, A.h, no),
+          :mpsb_normalize_lo_batch)
+    return no
+end
+
 function normalize_lo!(ctx::Ctx, A::DMPS)
     no = Ref{Cdouble}(0)
     check(ccall((:mpsb_normalize_lo, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Cdouble}), ctx.h, A.h, no),
