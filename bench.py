@@ -226,8 +226,8 @@ def run_op(argv):
         bench.py --op qr M N                     mpsb_op_qr (leftorth!/rightorth!, src/orthonormalisation.jl:164-234)
         bench.py --op gemm-mix [--chi --d --w]   prod_LR (3,4) / (4,3), update_re!, update_le! of one interior site
         bench.py --op zgemm M N K [--slices S]   mpsb_op_zgemm, FP64 (S=0) or int8-sliced tensor-core path
-        bench.py --op batch [--slices S]          steps of the batching workload, each inside an NVTX range
-                                                 "batch_step"
+        bench.py --op batch [CHI [T]] [--slices S]  steps of the batching workload (or of T trajectories of
+                                                 cap CHI), each inside an NVTX range "batch_step"
         bench.py --op rk4 [N] [--chi --w --slices S --random CHI0]
                                                  in-place RK4 steps of the density-matrix workload, each timed
                                                  step inside an NVTX range "rk4_step"
@@ -262,7 +262,7 @@ def run_op(argv):
         import numpy as np
         from mpsb200 import batch as BT, models as GM
         W = WORKLOADS["batch"]
-        chis = batch_chis(W)
+        chis = batch_chis(W) if not a.dims else [a.dims[0]] * (a.dims[1] if len(a.dims) > 1 else 16)
         n = a.warmup + a.reps
         u = [_uniforms(k, n) for k in range(len(chis))]
         tb = BT.TrajectoryBatch(GM.WaveguideChain(W["na"], omega=W["omega"]), chis, W["dt"],
