@@ -20,8 +20,10 @@
 //
 // Kernel (one 128 x 64 tile of C' per CTA, 256 threads): warp 0 issues TMA loads of the 2S
 // slice tiles of each 64-byte k-stage (64B swizzle) into a shared-memory ring, warp 1 owns the
-// TMEM allocation and one lane issues tcgen05.mma for all slice pairs of a stage and commits
-// the stage back to the producer, warps 4..7 are the epilogue (TMEM lanes 0..127).  Every wait
+// TMEM allocation and one lane issues tcgen05.mma for all slice pairs of a stage -- row i of
+// the slice triangle, A_i [B_0 .. B_{S-1-i}], as MMAs of N up to 256 whose output columns are
+// the consecutive level accumulators -- and commits the stage back to the producer, warps
+// 4..7 are the epilogue (TMEM lanes 0..127).  Every wait
 // is bounded in wall-clock time: a wait that runs out sets the context's error word and the CTA
 // winds down (copies in flight land, the TMEM allocation is released).
 #include <cuda.h>
@@ -105,19 +107,23 @@ __device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
   d |= (uint64_t)4 << 61;                        // layout: 64-byte swizzle
   return d;
 }
-// instruction descriptor: kind::i8, signed A and B, s32 accumulator, both K-major, M=128, N=64
-__host__ __device__ constexpr uint32_t idesc_i8() {
-  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+// instruction descriptor: kind::i8, signed A and B, s32 accumulator, both K-major, M=128, N=n
+// (a multiple of 16 up to 256)
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
 }
+// B slices one MMA covers: N = OZ_BN per slice, at most 256
+constexpr int OZ_SLICES_PER_MMA = 256 / OZ_BN;
 // A-operand collector use across consecutive MMAs that share A: 0 = read A (no reuse),
 // 1 = read and keep it, 2 = reuse the kept A, 3 = reuse it for the last time
 #define MPSB_MMA_I8(QUAL)                                                                          \
   asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"                                        \
                "tcgen05.mma.cta_group::1.kind::i8" QUAL " [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d), \
-               "l"(adesc), "l"(bdesc), "r"(idesc_i8()), "r"(accumulate)                             \
+               "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)                                  \
                : "memory")
 template <int COLLECT>
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
   if (COLLECT == 1) MPSB_MMA_I8(".collector::a::fill");
   else if (COLLECT == 2) MPSB_MMA_I8(".collector::a::use");
   else if (COLLECT == 3) MPSB_MMA_I8(".collector::a::lastuse");
@@ -351,17 +357,27 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         for (int kk = 0; kk < OZ_BK / 32; ++kk) {
 #pragma unroll
           for (int i = 0; i < S; ++i) {
+            // Row i of the slice triangle: A_i times B_0 .. B_{S-1-i}.  The B slice tiles of a
+            // stage are consecutive 64-row blocks of one swizzled operand, and the level
+            // accumulators are consecutive OZ_BN-column blocks of TMEM, so A_i [B_j .. B_{j+n-1}]
+            // is one MMA with N = n * OZ_BN whose output columns start at level i + j: the
+            // products land in their levels without any per-level MMA.
             const uint64_t ad = smem_desc_sw64(st + i * A_TILE + kk * 32);
+            const int nmma = (S - i + OZ_SLICES_PER_MMA - 1) / OZ_SLICES_PER_MMA;
 #pragma unroll
-            for (int j = 0; j < S - i; ++j) {
+            for (int q = 0; q < (S + OZ_SLICES_PER_MMA - 1) / OZ_SLICES_PER_MMA; ++q) {
+              if (q >= nmma) break;
+              const int j = q * OZ_SLICES_PER_MMA;
+              const int nj = (S - i - j) < OZ_SLICES_PER_MMA ? (S - i - j) : OZ_SLICES_PER_MMA;
               const uint64_t bd = smem_desc_sw64(st + S * A_TILE + j * B_TILE + kk * 32);
               const uint32_t acc = (kb > 0 || kk > 0 || i > 0) ? 1u : 0u;   // i == 0 opens every level
               const uint32_t td = tmem + (uint32_t)((i + j) * OZ_BN);
-              // A_i is shared by the S - i products of this row of the slice triangle
-              if (S - i == 1) mma_i8<0>(td, ad, bd, acc);
-              else if (j == 0) mma_i8<1>(td, ad, bd, acc);
-              else if (j == S - i - 1) mma_i8<3>(td, ad, bd, acc);
-              else mma_i8<2>(td, ad, bd, acc);
+              const uint32_t id = idesc_i8(nj * OZ_BN);
+              // A_i is shared by the nmma products of this row
+              if (nmma == 1) mma_i8<0>(td, ad, bd, id, acc);
+              else if (q == 0) mma_i8<1>(td, ad, bd, id, acc);
+              else if (q == nmma - 1) mma_i8<3>(td, ad, bd, id, acc);
+              else mma_i8<2>(td, ad, bd, id, acc);
             }
           }
         }
