@@ -39,11 +39,12 @@ static int sync(mpsb_ctx* ctx) {
   MPSB_CUDA_TRY(cudaMemcpyAsync(hw, ctx->err(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   MPSB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   if (*hw != 0) {
+    const int word = *hw;
     *hw = 0;
     cudaMemsetAsync(ctx->err(), 0, sizeof(int), ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     set_last_message("a device-side wait timed out (%s); results of this stream are invalid",
-                     (*hw & 4) ? "wait self-test" : (*hw & 2) ? "sliced GEMM pipeline" : "QR cluster exchange");
+                     (word & 4) ? "wait self-test" : (word & 2) ? "sliced GEMM pipeline" : "QR cluster exchange");
     return MPSB_ERR_CUDA;
   }
   return MPSB_OK;

@@ -168,7 +168,7 @@ def test_bounded_wait_runs_out_and_the_context_recovers(gpu_ctx):
     t0 = time.perf_counter()
     with pytest.raises(_lib.MpsbError) as e:
         _lib.call("mpsb_wait_selftest", gpu_ctx.h, 0.05)
-    assert e.value.status == -3 and "timed out" in str(e.value)
+    assert e.value.status == -3 and "timed out" in str(e.value) and "wait self-test" in str(e.value)
     assert time.perf_counter() - t0 < 5.0
     rng = np.random.default_rng(12)
     A, B = crand(rng, 96, 64), crand(rng, 64, 40)
