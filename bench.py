@@ -191,18 +191,27 @@ def job_rate(world, sites, steps, secs):
 
 
 def run_serving():
-    """p50/p99 job latency of a bounded sample of the mixed serving stream: 24 seeded Poisson
-    arrivals at 200 jobs/s, 70% trajectories (N 20..40, chi 16/32/64, d=2, w=4) and 30%
-    density matrices (N 8..16, chi 16/32, d=4, w=8), 10..30 RK4 steps each, up to 8 jobs on the
-    device at once (the configuration's full sizes and 100-500 steps would run for minutes)."""
+    """p50/p99 job latency of a bounded sample of the mixed serving stream with the configuration's
+    size ranges: 24 seeded Poisson arrivals at 200 jobs/s, 70% trajectories (N 20..100, d=2, w=4,
+    chi in {32, 64, 128, 256, 512}) and 30% density matrices (N 20..60, d=4, w=8, chi in {64, 128,
+    256}), 3..6 RK4 steps each (the configuration's 100..500 would run for many minutes), up to 16
+    jobs on the device in shared buckets of the batched engine (continuous batching, 6 int8
+    slices for the larger contractions)."""
     from mpsb200 import serve as S
-    jobs = S.poisson_jobs(24, 200.0, 11)
-    done, st = S.Server(max_jobs=8).run(jobs)
-    return {"jobs": st["jobs"], "arrival_rate_per_s": 200.0, "slots": 8,
+    jobs = S.poisson_jobs(24, 200.0, 11, traj_na=(20, 100), traj_chi=(32, 64, 128, 256, 512), rho_na=(20, 60),
+                          rho_chi=(64, 128, 256), steps=(3, 6))
+    buckets = {}
+
+    def seen(sl):
+        buckets.setdefault(id(sl.bucket), []).append(sl.job.job_id)
+
+    done, st = S.Server(max_jobs=16, slots=8, slices=6).run(jobs, on_admit=seen)
+    return {"jobs": st["jobs"], "arrival_rate_per_s": 200.0, "max_running": 16, "mode": "shared buckets",
+            "buckets": len(buckets), "jobs_per_bucket_max": max(len(v) for v in buckets.values()),
             "latency_p50_ms": 1e3 * st["latency_p50_s"], "latency_p99_ms": 1e3 * st["latency_p99_s"],
             "queue_p50_ms": 1e3 * st["queue_p50_s"], "site_updates_per_s": st["site_updates_per_s"],
-            "wall_s": st["wall_s"],
-            "sample": "24 jobs: 70% trajectories N 20..40 chi<=64, 30% rho N 8..16 chi<=32, 10..30 steps"}
+            "wall_s": st["wall_s"], "failed": len(st["failed"]), "refused": len(st["refused"]),
+            "sample": "24 jobs: 70% trajectories N 20..100 chi 32..512, 30% rho N 20..60 chi 64..256, 3..6 steps"}
 
 
 def _event_us(torch, stream, fn, reps, warmup, ctx):

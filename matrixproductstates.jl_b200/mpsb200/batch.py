@@ -42,8 +42,13 @@ class TrajectoryBucket:
 
     def __init__(self, p, chi, dt, r1, r2, device=0, ctx=None, slices=0):
         self.p, self.chi, self.dt = p, int(chi), dt
-        self.r1, self.r2 = np.atleast_2d(r1), np.atleast_2d(r2)      # [copy, step]
-        self.B = self.r1.shape[0]
+        # every copy's own uniform streams and step index (copies may start at different steps
+        # when a serving loop hands a slot to a new job, see assign)
+        self.r1 = [np.asarray(x, dtype=np.float64) for x in np.atleast_2d(r1)]
+        self.r2 = [np.asarray(x, dtype=np.float64) for x in np.atleast_2d(r2)]
+        self.B = len(self.r1)
+        self.t = np.zeros(self.B, dtype=np.int64)
+        self.active = np.ones(self.B, dtype=bool)
         self.ctx = ctx or K.Context(device)
         self.own_ctx = ctx is None
         self.ctx.set_precision(slices)
@@ -55,7 +60,8 @@ class TrajectoryBucket:
         # mpsgroundstate (src/constructors.jl:67-76): the padded product state left-orthogonalised
         # by the QR sweep (its zero-weight columns are the Householder ones), in every copy
         start, _ = K.mpsgroundstate(na, self.chi, 2, c)
-        for k, site in enumerate(start.sites()):
+        self.start_sites = start.sites()
+        for k, site in enumerate(self.start_sites):
             for b in range(B):
                 self.A.set_site_copy(b, k, site)
         del start
@@ -79,27 +85,56 @@ class TrajectoryBucket:
         for mpo, sites in zip(self.H, host_sites):
             mpo.set_sites(sites)
 
+    def assign(self, b, r1, r2):
+        """Give copy b to a new trajectory: the start state, its own uniform streams, step 0."""
+        self.reset(b)
+        self.r1[b], self.r2[b] = np.asarray(r1, dtype=np.float64), np.asarray(r2, dtype=np.float64)
+        self.t[b] = 0
+        self.p_coh[b], self.jumps[b] = [], []
+        self.active[b] = True
+
+    def release(self, b):
+        """Copy b keeps being stepped with the others but carries no trajectory."""
+        self.active[b] = False
+
+    def reset(self, b):
+        """Copy b <- the start state (a released copy whose state went bad)."""
+        for k, site in enumerate(self.start_sites):
+            self.A.set_site_copy(b, k, site)
+
+    def state(self, b):
+        return self.A.sites_copy(b)
+
     def issue(self):
         """Enqueue step i's coherent step for every copy (no wait)."""
         K.RK4stp_apply_H_half_(self.dt, self.H, self.A_coh, self.A, self.A1, self.A2, self.A3,
                                self.env1, self.env2, self.env3, self.envop)
 
-    def finish(self):
-        """Norms, per-trajectory decisions of step i, and the state update A <- chosen copy."""
-        i, p, dt, na = self.i, self.p, self.dt, self.p.na
-        p_coh = K.normalize_lo_batch(self.A_coh)
+    def finish(self, bad=None):
+        """Norms, each active trajectory's decision of its own step, and the state update
+        A <- chosen copy.  With `bad` (a list), a copy whose norm is not finite is appended to it
+        and released instead of raising (a serving loop fails that job alone)."""
+        p, dt, na = self.p, self.dt, self.p.na
+        p_coh = K.normalize_lo_batch(self.A_coh, allow_nonfinite=bad is not None)
+        if bad is not None:
+            for b in range(self.B):
+                if self.active[b] and not (np.isfinite(p_coh[b]) and p_coh[b] <= 1e300):
+                    bad.append(b)
+                    self.active[b] = False
+        act = [b for b in range(self.B) if self.active[b]]
         p_r = p_l = None
-        if np.any(self.r1[:, i] >= p_coh):   # a jump step for some copy
+        if any(self.r1[b][self.t[b]] >= p_coh[b] for b in act):   # a jump step for some copy
             K.compress_var_apply_H_(self.A_r, self.envop_jump, self.A, self.A, self.jumpright, 1)
             p_r = K.normalize_lo_batch(self.A_r)
             K.compress_var_apply_H_(self.A_l, self.envop_jump, self.A, self.A, self.jumpleft, 1)
             p_l = K.normalize_lo_batch(self.A_l)
-        which = np.full(self.B, -1, dtype=np.int64)
+        which = np.zeros(self.B, dtype=np.int64)   # released copies keep their coherent step
         local = []
-        for b in range(self.B):
+        for b in act:
+            i = int(self.t[b])
+            self.t[b] += 1
             self.p_coh[b].append(p_coh[b])
-            if self.r1[b, i] < p_coh[b]:
-                which[b] = 0
+            if self.r1[b][i] < p_coh[b]:
                 continue
             p_acc = np.zeros(na + 3)
             if p.gam_eg != 0:
@@ -110,8 +145,9 @@ class TrajectoryBucket:
             p_acc[na + 2] = p_acc[na + 1] + dt * p_l[b]
             p_sum = p_acc[-1]
             p_acc = p_acc / p_acc[-1]
-            r = self.r2[b, i]
+            r = self.r2[b][i]
             if r < p_acc[na]:
+                which[b] = -1   # the local decay acts on the step's start state
                 for j in range(na):
                     if r < p_acc[j + 1]:
                         local.append((b, j))
@@ -133,6 +169,65 @@ class TrajectoryBucket:
     def close(self):
         for name in ("A", "A_coh", "A_r", "A_l", "A1", "A2", "A3", "envop", "envop_jump", "env1", "env2", "env3",
                      "H", "jumpright", "jumpleft"):
+            setattr(self, name, None)
+        if self.own_ctx:
+            self.ctx.close()
+
+
+class DensityBucket:
+    """Density-matrix evolutions of one shape (N, chi, w, dt) in the copies of batch handles: the
+    in-place RK4 step of examples/spin_model_density_matrix.jl for every copy in one call.  Copies
+    are handed to jobs (assign) and given back (release) by a serving loop; each copy counts its
+    own steps."""
+
+    def __init__(self, p, chi, dt, B, w=8, device=0, ctx=None, slices=0):
+        self.p, self.chi, self.dt, self.B, self.w = p, int(chi), dt, int(B), int(w)
+        self.ctx = ctx or K.Context(device)
+        self.own_ctx = ctx is None
+        self.ctx.set_precision(slices)
+        na, c = p.na, self.ctx
+        dims = dims_rule(na, self.chi, 4)
+        self.dims = dims
+        start, _ = K.mpsgroundstate(na, self.chi, 4, c)
+        self.start_sites = start.sites()
+        del start
+        self.rho, self.rho1, self.rho2, self.rho3 = (K.MPS(dims, 4, c, batch=self.B) for _ in range(4))
+        for b in range(self.B):
+            self.reset(b)
+        self.env1, self.env2, self.env3 = (K.build_env(dims, dims, None, c, batch=self.B) for _ in range(3))
+        self.envop = K.build_env(dims, dims, [max(6, self.w)] * (na + 1), c, batch=self.B)
+        self.L = [K.MPO.from_sites(Mo.construct_L_spin_model(p, 1, dt / 2, 0.0, self.w), c),
+                  K.MPO.from_sites(Mo.construct_L_spin_model(p, 0, 1, dt / 2, self.w), c),
+                  K.MPO.from_sites(Mo.construct_L_spin_model(p, 1, dt / 2, dt, self.w), c)]
+        self.t = np.zeros(self.B, dtype=np.int64)
+        self.active = np.zeros(self.B, dtype=bool)
+
+    def reset(self, b):
+        """Copy b <- the all-down product density matrix (mpsgroundstate with d = 4)."""
+        for k, site in enumerate(self.start_sites):
+            self.rho.set_site_copy(b, k, site)
+
+    def assign(self, b):
+        self.reset(b)
+        self.t[b] = 0
+        self.active[b] = True
+
+    def release(self, b):
+        self.active[b] = False
+
+    def issue(self):
+        """Enqueue one in-place RK4 step of every copy (no wait)."""
+        K.RK4stp_apply_H_half_(self.dt, self.L, self.rho, self.rho1, self.rho2, self.rho3,
+                               self.env1, self.env2, self.env3, self.envop)
+
+    def finish(self, bad=None):
+        self.t[self.active] += 1
+
+    def state(self, b):
+        return self.rho.sites_copy(b)
+
+    def close(self):
+        for name in ("rho", "rho1", "rho2", "rho3", "env1", "env2", "env3", "envop", "L"):
             setattr(self, name, None)
         if self.own_ctx:
             self.ctx.close()

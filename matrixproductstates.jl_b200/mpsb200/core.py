@@ -695,10 +695,16 @@ def normalize_lo_(mps):
     return _scalar("mpsb_normalize_lo", mps.ctx.h, mps.h)
 
 
-def normalize_lo_batch(mps):
-    """normalize_lo! of every copy of a batch handle; returns the norms^2 before scaling."""
+def normalize_lo_batch(mps, allow_nonfinite=False):
+    """normalize_lo! of every copy of a batch handle; returns the norms^2 before scaling.  A copy
+    whose norm is NaN or infinite raises MPSB_ERR_NONFINITE, unless allow_nonfinite, which returns
+    the norms as they are (the caller checks each copy)."""
     out = np.zeros(mps.batch, dtype=np.float64)
-    _lib.call("mpsb_normalize_lo_batch", mps.ctx.h, mps.h, _dptr(out))
+    try:
+        _lib.call("mpsb_normalize_lo_batch", mps.ctx.h, mps.h, _dptr(out))
+    except _lib.MpsbError as e:
+        if not (allow_nonfinite and e.status == -6):
+            raise
     return out
 
 

@@ -65,9 +65,9 @@ def test_a_failing_job_leaves_the_others_intact(gpu_ctx):
         if a.job.job_id == bad:
             a.buf.H[0].set_site(0, a.buf.H[0].site(0) * np.nan)
 
-    mixed, stats = S.Server(max_jobs=3).run(jobs, keep_results=True, on_admit=corrupt)
+    mixed, stats = S.Server(max_jobs=3, mode="per_job").run(jobs, keep_results=True, on_admit=corrupt)
     assert [f["job_id"] for f in stats["failed"]] == [bad] and "NONFINITE" in stats["failed"][0]["error"]
-    clean, _ = S.Server(max_jobs=3).run([j for j in jobs if j.job_id != bad], keep_results=True)
+    clean, _ = S.Server(max_jobs=3, mode="per_job").run([j for j in jobs if j.job_id != bad], keep_results=True)
     assert sorted(r["job_id"] for r in mixed) == sorted(r["job_id"] for r in clean)
     for r in mixed:
         c = next(x for x in clean if x["job_id"] == r["job_id"])
@@ -79,13 +79,77 @@ def test_results_are_the_same_alone_and_in_the_mix(gpu_ctx):
     from mpsb200 import serve as S
     jobs = S.poisson_jobs(6, 200.0, 3, traj_na=(10, 14), traj_chi=(8, 16), rho_na=(6, 8), rho_chi=(8, 16),
                           steps=(6, 12))
-    mix, stats = S.Server(max_jobs=4).run(jobs, keep_results=True)
+    mix, stats = S.Server(max_jobs=4, mode="per_job").run(jobs, keep_results=True)
     assert stats["jobs"] == len(jobs)
     assert stats["latency_p99_s"] >= stats["latency_p50_s"] > 0
     for r in mix:
         job = next(j for j in jobs if j.job_id == r["job_id"])
-        alone, _ = S.Server(max_jobs=1).run([dataclasses.replace(job, arrival=0.0)], keep_results=True)
+        alone, _ = S.Server(max_jobs=1, mode="per_job").run([dataclasses.replace(job, arrival=0.0)],
+                                                             keep_results=True)
         a = alone[0]
         assert all(np.array_equal(x, y) for x, y in zip(r["state"], a["state"]))
         if r["kind"] == "trajectory":
             assert r["jumps"] == a["jumps"] and np.array_equal(r["p_coh"], a["p_coh"])
+
+
+def _shape_mix(n, seed):
+    """A stream whose jobs repeat a few shapes, so shared buckets hold several jobs at once and
+    jobs join a bucket that is already running (later arrivals, other step counts)."""
+    from mpsb200 import serve as S
+    rng = np.random.default_rng(seed)
+    shapes = [("trajectory", 10, 16, 0.01), ("trajectory", 12, 8, 0.01), ("density", 6, 16, 0.005)]
+    jobs, t = [], 0.0
+    for i in range(n):
+        kind, na, chi, dt = shapes[int(rng.integers(len(shapes)))]
+        t += rng.exponential(1.0 / 400.0)
+        jobs.append(S.Job(kind, na, chi, int(rng.integers(5, 12)), dt, 1000 + i, t, i))
+    return jobs
+
+
+@pytest.mark.gpu
+def test_shared_buckets_results_are_the_same_alone_and_in_the_mix(gpu_ctx):
+    """Continuous batching: jobs of one shape share the batched engine's bucket, join it while it
+    runs, and leave it at their own step count; every job's state, jump record and norms are
+    bitwise those of the job run alone."""
+    from mpsb200 import serve as S
+    jobs = _shape_mix(12, 21)
+    shared = {}
+
+    def seen(sl):
+        shared.setdefault(id(sl.bucket), set()).add(sl.job.job_id)
+
+    mix, stats = S.Server(max_jobs=8, slots=4).run(jobs, keep_results=True, on_admit=seen)
+    assert stats["jobs"] == len(jobs) and stats["failed"] == [] and stats["refused"] == []
+    assert max(len(v) for v in shared.values()) >= 3       # some bucket carried several jobs
+    for r in mix:
+        job = next(j for j in jobs if j.job_id == r["job_id"])
+        alone, _ = S.Server(max_jobs=1, slots=4).run([dataclasses.replace(job, arrival=0.0)], keep_results=True)
+        a = alone[0]
+        assert all(np.array_equal(x, y) for x, y in zip(r["state"], a["state"]))
+        if r["kind"] == "trajectory":
+            assert r["jumps"] == a["jumps"] and np.array_equal(r["p_coh"], a["p_coh"])
+
+
+@pytest.mark.gpu
+def test_shared_bucket_failing_trajectory_leaves_its_bucket_mates_intact(gpu_ctx):
+    """Fault injected from the host: one trajectory's copy in a shared bucket gets a NaN site
+    after admission.  Its norm is not finite, so that job fails and its slot is reset; the jobs
+    sharing the bucket finish with the results they have without it."""
+    from mpsb200 import serve as S
+    jobs = [S.Job("trajectory", 10, 16, 8, 0.01, 500 + i, 0.0, i) for i in range(4)]
+    bad = 2
+
+    def corrupt(sl):
+        if sl.job.job_id == bad:
+            site = sl.bucket.eng.A.site_copy(sl.slot, 3)
+            sl.bucket.eng.A.set_site_copy(sl.slot, 3, site * np.nan)
+
+    mixed, stats = S.Server(max_jobs=4, slots=4).run(jobs, keep_results=True, on_admit=corrupt)
+    assert [(f["job_id"], f["step"]) for f in stats["failed"]] == [(bad, 0)]
+    assert "NONFINITE" in stats["failed"][0]["error"]
+    clean, _ = S.Server(max_jobs=4, slots=4).run([j for j in jobs if j.job_id != bad], keep_results=True)
+    assert sorted(r["job_id"] for r in mixed) == sorted(r["job_id"] for r in clean) == [0, 1, 3]
+    for r in mixed:
+        c = next(x for x in clean if x["job_id"] == r["job_id"])
+        assert all(np.array_equal(x, y) for x, y in zip(r["state"], c["state"]))
+        assert np.array_equal(r["p_coh"], c["p_coh"]) and r["jumps"] == c["jumps"]
