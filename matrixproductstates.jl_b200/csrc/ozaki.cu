@@ -29,6 +29,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -159,26 +160,37 @@ struct SliceView {
 };
 
 // biased IEEE exponent of max(|re|, |im|) (0 for zero / subnormal), max-reduced per row into
-// rexp (zeroed before)
-__global__ void oz_rowexp_kernel(SliceView v, int* __restrict__ rexp0, int64_t rexp_bat) {
+// rexp (zeroed before).  A CTA covers 32 rows and kper tiles of 32 columns, keeping a running
+// maximum per thread: for large operands several loads per thread are in flight and one atomic
+// per row and CTA remains, small ones keep one tile per CTA and the grid wide.
+__global__ void oz_rowexp_kernel(SliceView v, int* __restrict__ rexp0, int64_t rexp_bat, int kper) {
   __shared__ int tile_e[32][33];
-  const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int r0 = blockIdx.x * 32;
   v.X += (int64_t)blockIdx.z * v.x_bat;
   int* rexp = rexp0 + (int64_t)blockIdx.z * rexp_bat;
   const int tid = threadIdx.x;
   const bool rc = (v.x_r == 1);   // rows contiguous: lanes run along r
-  for (int i = 0; i < 4; ++i) {
-    int rr, kk;
-    if (rc) { rr = tid % 32; kk = tid / 32 + 8 * i; }
-    else    { kk = tid % 32; rr = tid / 32 + 8 * i; }
-    const int r = r0 + rr, k = k0 + kk;
-    int e = 0;
-    if (r < v.R && k < v.K) {
-      const cd x = v.X[(int64_t)r * v.x_r + (int64_t)k * v.x_k];
-      const double m = fmax(fabs(x.x), fabs(x.y));
-      e = (int)((__double_as_longlong(m) >> 52) & 0x7FF);
+  const int kt0 = blockIdx.y * kper, kt1 = min((v.K + 31) / 32, kt0 + kper);
+  int em[4] = {0, 0, 0, 0};
+#pragma unroll 2
+  for (int kt = kt0; kt < kt1; ++kt) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int rr, kk;
+      if (rc) { rr = tid % 32; kk = tid / 32 + 8 * i; }
+      else    { kk = tid % 32; rr = tid / 32 + 8 * i; }
+      const int r = r0 + rr, k = kt * 32 + kk;
+      if (r < v.R && k < v.K) {
+        const cd x = v.X[(int64_t)r * v.x_r + (int64_t)k * v.x_k];
+        const double m = fmax(fabs(x.x), fabs(x.y));
+        em[i] = max(em[i], (int)((__double_as_longlong(m) >> 52) & 0x7FF));
+      }
     }
-    tile_e[rr][kk] = e;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (rc) tile_e[tid % 32][tid / 32 + 8 * i] = em[i];
+    else    tile_e[tid / 32 + 8 * i][tid % 32] = em[i];
   }
   __syncthreads();
   const int warp = tid / 32, lane = tid % 32;
@@ -189,22 +201,40 @@ __global__ void oz_rowexp_kernel(SliceView v, int* __restrict__ rexp0, int64_t r
   }
 }
 
+// 2^k for -1022 <= k <= 1023, written into the exponent field
+__device__ __forceinline__ double pow2_exact(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
+// The scaling x -> x 2^(7-e) of a row whose maximum has the biased exponent E (e = E - 1022, its
+// frexp exponent) as two exact multiplications x * s1 * s2 (2^(7-e) itself overflows for E < 6);
+// a row of zeros and subnormals (E = 0) gets s2 = 0.
+struct RowScale {
+  double s1, s2;
+};
+__device__ __forceinline__ RowScale row_scale(int E) {
+  const int k = 1029 - E;
+  RowScale r;
+  r.s1 = (k > 1023) ? pow2_exact(512) : 1.0;
+  r.s2 = (E > 0) ? pow2_exact(k > 1023 ? k - 512 : k) : 0.0;
+  return r;
+}
+
+// Balanced base-128 digits of x 2^(7-e) in (-128, 128): d_i = round-to-nearest-even of the
+// remainder clamped to [-127, 127], every step exact in FP64.  The clamp matters at every digit:
+// x just below a power of two (1 - 1e-12, say) gives a run of remainders in (127, 128).
 template <int S>
-__device__ __forceinline__ void digits(double x, int E, int (&d)[S]) {
-  // x 2^(7-e) in (-128, 128) with e the frexp exponent of the row maximum; every step below is
-  // exact in FP64
-  double t = (E > 0) ? ldexp(x, 7 - (E - 1022)) : 0.0;
+__device__ __forceinline__ void digits(double x, RowScale rs, int (&d)[S]) {
+  double t = (x * rs.s1) * rs.s2;
 #pragma unroll
   for (int i = 0; i < S; ++i) {
-    const double q = fmin(fmax(rint(t), -127.0), 127.0);
-    d[i] = (int)q;
-    t = (t - q) * 128.0;
+    const int q = max(-127, min(127, __double2int_rn(t)));
+    d[i] = q;
+    if (i + 1 < S) t = (t - (double)q) * 128.0;
   }
 }
 
 __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
-  return (uint32_t)(uint8_t)a | ((uint32_t)(uint8_t)b << 8) | ((uint32_t)(uint8_t)c << 16) |
-         ((uint32_t)(uint8_t)d << 24);
+  // the low bytes of a, b, c, d (their int8 values) as bytes 0..3
+  return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
 // Digits of a 32-row x 32-complex tile: out[t][row][k'] (K' = 2K padded to Kp, rows padded to
@@ -235,13 +265,13 @@ __global__ void oz_split_kernel(SliceView v, const int* __restrict__ rexp0, int6
   // thread -> (row, 4 consecutive complex k)
   const int rr = tid / 8, kq = (tid % 8) * 4;
   const int r = r0 + rr;
-  const int E = (r < v.R) ? rexp[r] : 0;
+  const RowScale rs = row_scale((r < v.R) ? rexp[r] : 0);
   int dre[4][S], dim[4][S];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const cd x = tile[rr][kq + j];
-    digits<S>(x.x, E, dre[j]);
-    digits<S>(x.y, E, dim[j]);
+    digits<S>(x.x, rs, dre[j]);
+    digits<S>(x.y, rs, dim[j]);
   }
   const int64_t kbyte = 2 * (int64_t)(k0 + kq);   // first k' of this thread (8 bytes, < Kp)
 #pragma unroll
@@ -385,23 +415,28 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       }
       mma_commit(accum);         // every MMA of this CTA done (also on the abort path)
     }
-  } else if (warp >= 4) {
-    // ---- epilogue: TMEM lanes 32*(warp-4) .. +31 are rows m0 + 32*(warp-4) + lane
+  }
+  // ---- epilogue, all eight warps once the accumulators are complete: warp w reads TMEM lanes
+  // 32*(w%4) .. +31 (rows m0 + 32*(w%4) + lane, the lane quarter a warp may access) and the
+  // 32-column half w/4 of every level
+  __syncwarp();
+  {
+    const int quarter = warp % 4, half = warp / 4;
     bool ok = true;
     if (lane == 0) ok = mbar_wait(accum, 0);   // one poller per warp
     ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
     fence_after();
     if (!ok) *abort_flag = 1;
-    const int row = 32 * (warp - 4) + lane;
+    const int row = 32 * quarter + lane;
     const int m = m0 + row;
-    const uint32_t tbase = tmem + ((uint32_t)(32 * (warp - 4)) << 16);
+    const uint32_t tbase = tmem + ((uint32_t)(32 * quarter) << 16);
     const int Ea = P.ea[(int64_t)prob * P.Mpad + m];
     const int* eb = P.eb + (int64_t)prob * (P.NBpad / 2);
     cd* Cp = P.C + (int64_t)prob * P.c_bat;
     const bool use_beta = (P.beta.x != 0.0) || (P.beta.y != 0.0);
     const bool good = ok && !*abort_flag;
-#pragma unroll 1
-    for (int half = 0; half < OZ_BN / 32; ++half) {
+    static_assert(OZ_BN == 64, "two 32-column halves, one per group of four warps");
+    {
       double acc[32];
 #pragma unroll
       for (int c = 0; c < 32; ++c) acc[c] = 0.0;
@@ -410,7 +445,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         int v[32];
         __syncwarp();   // tcgen05.ld is warp-collective
         tmem_ld32(tbase + (uint32_t)(t * OZ_BN + half * 32), v);
-        const double w = ldexp(1.0, -7 * (t + 2));
+        const double w = pow2_exact(-7 * (t + 2));
 #pragma unroll
         for (int c = 0; c < 32; ++c) acc[c] += (double)v[c] * w;
       }
@@ -424,8 +459,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             double re = 0.0, im = 0.0;
             if (Ea > 0 && Eb > 0) {
               const int e = (Ea - 1022) + (Eb - 1022);
-              re = ldexp(acc[2 * c], e);
-              im = ldexp(acc[2 * c + 1], e);
+              if (e >= -1022 && e <= 1023) {   // one exact power-of-two multiply, as ldexp rounds
+                const double sc = pow2_exact(e);
+                re = acc[2 * c] * sc;
+                im = acc[2 * c + 1] * sc;
+              } else {
+                re = ldexp(acc[2 * c], e);
+                im = ldexp(acc[2 * c + 1], e);
+              }
             }
             cd* cp = Cp + (int64_t)m * P.c_m + (int64_t)n * P.c_n;
             cd val = cmul(P.alpha, cmk(re, im));
@@ -584,11 +625,20 @@ int ozgemm_launch(const Gemm& g, int slices, void* scratch, size_t scratch_bytes
   const int kc = (int)(Kp / 2);   // complex k extent covered by the slice grid
   const unsigned bz = (unsigned)B;
   count_launch(ws);
-  oz_rowexp_kernel<<<dim3((unsigned)((g.M + 31) / 32), (unsigned)((g.K + 31) / 32), bz), 256, 0, s>>>(va, ea, Mpad);
+  // k tiles per exponent-scan CTA: up to 8 while the grid stays above 8 CTAs per SM (the maximum
+  // is the same whatever the partition)
+  const int ktiles = (g.K + 31) / 32;
+  auto kper = [&](int rows) {
+    const int64_t tiles = (int64_t)((rows + 31) / 32) * ktiles * B;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(8, tiles / (148 * 8)));
+  };
+  const int ka = kper(g.M), kb = kper(g.N);
+  oz_rowexp_kernel<<<dim3((unsigned)((g.M + 31) / 32), (unsigned)((ktiles + ka - 1) / ka), bz), 256, 0, s>>>(
+      va, ea, Mpad, ka);
   MPSB_CUDA_TRY(cudaGetLastError());
   count_launch(ws);
-  oz_rowexp_kernel<<<dim3((unsigned)((g.N + 31) / 32), (unsigned)((g.K + 31) / 32), bz), 256, 0, s>>>(vb, eb,
-                                                                                                      NBpad / 2);
+  oz_rowexp_kernel<<<dim3((unsigned)((g.N + 31) / 32), (unsigned)((ktiles + kb - 1) / kb), bz), 256, 0, s>>>(
+      vb, eb, NBpad / 2, kb);
   MPSB_CUDA_TRY(cudaGetLastError());
   count_launch(ws);
   pick_split(S, false)<<<dim3((unsigned)(Mpad / 32), (unsigned)(kc / 32), bz), 256, 0, s>>>(va, ea, Mpad, sa, Mpad,
