@@ -18,14 +18,17 @@
 //   * the epilogue reads the S accumulators, sums them in FP64 from the smallest weight up,
 //     applies 2^(E_a + E_b), alpha and beta, and writes complex128 C through its strides.
 //
-// Kernel (one 128 x 64 tile of C' per CTA, 256 threads): warp 0 issues TMA loads of the 2S
-// slice tiles of each 64-byte k-stage (64B swizzle) into a shared-memory ring, warp 1 owns the
-// TMEM allocation and one lane issues tcgen05.mma for all slice pairs of a stage -- row i of
-// the slice triangle, A_i [B_0 .. B_{S-1-i}], as MMAs of N up to 256 whose output columns are
-// the consecutive level accumulators -- and commits the stage back to the producer, warps
-// 4..7 are the epilogue (TMEM lanes 0..127).  Every wait
-// is bounded in wall-clock time: a wait that runs out sets the context's error word and the CTA
-// winds down (copies in flight land, the TMEM allocation is released).
+// Kernel (persistent: one CTA per SM, 384 threads, 128 x 64 tiles of C' of every problem taken
+// round-robin): warp 0 issues TMA loads of the 2S slice tiles of each 64-byte k-stage (64B
+// swizzle) into a shared-memory ring that runs on across tiles; warp 1 owns the TMEM allocation
+// and one lane issues tcgen05.mma for all slice pairs of a stage -- row i of the slice triangle,
+// A_i [B_0 .. B_{S-1-i}], as MMAs of N up to 256 whose output columns are the consecutive level
+// accumulators -- and commits the stage back to the producer; warps 4..11 are the epilogue (two
+// warps per TMEM lane quarter, one 32-column half each), which hands the accumulators back as
+// soon as it has read them, so the next tile's loads and MMAs overlap its FP64 combination and
+// stores.  Every wait is bounded in wall-clock time: a wait that runs out sets the context's
+// error word and the CTA winds down (copies in flight land, no MMA is left running, the TMEM
+// allocation is released).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -46,7 +49,8 @@ constexpr int OZ_BK = 64;         // int8 k per stage: one 64-byte swizzled row
 constexpr int OZ_KP_ALIGN = 64;   // K' padding
 constexpr int A_TILE = OZ_BM * OZ_BK;   // 8 KB
 constexpr int B_TILE = OZ_BN * OZ_BK;   // 4 KB
-constexpr int OZ_THREADS = 256;
+constexpr int OZ_THREADS = 384;   // warp 0 TMA, warp 1 TMEM + MMA, warps 2-3 idle, warps 4-11 epilogue
+constexpr int OZ_EPI_WARPS = 8;
 constexpr unsigned long long WAIT_NS = 2000000000ull;   // a bounded mbarrier wait gives up after 2 s
 
 __host__ __device__ constexpr int stage_bytes(int S) { return S * (A_TILE + B_TILE); }
@@ -65,6 +69,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 // non-blocking test of the phase of the given parity
 __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
@@ -300,8 +307,8 @@ struct OzParams {
   cd* C; int64_t c_m, c_n, c_bat;
   cd alpha, beta;
   int* err;              // device error word (bit 1: a wait in this kernel ran out)
-  // problem blockIdx.y of a batch: its slices start at row blockIdx.y * S * Mpad (* NBpad) of
-  // the tensor maps, its exponents at blockIdx.y * Mpad (* NBpad / 2)
+  int nprob;             // problems of the batch: problem p's slices start at row p * S * Mpad
+                         // (* NBpad) of the tensor maps, its exponents at p * Mpad (* NBpad / 2)
 };
 
 template <int S>
@@ -314,16 +321,24 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * SB);
   uint64_t* empty = full + ST;
-  uint64_t* accum = empty + ST;
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(accum + 1);
+  uint64_t* accum = empty + ST;      // the MMAs of a tile are complete (one commit per tile)
+  uint64_t* drained = accum + 1;     // the epilogue has read a tile's accumulators (8 warps arrive)
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drained + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int tiles_m = P.Mpad / OZ_BM;
-  const int m_tile = blockIdx.x % tiles_m, n_tile = blockIdx.x / tiles_m;
-  const int m0 = m_tile * OZ_BM, n0 = n_tile * OZ_BN;   // n0 in real columns of C'
-  const int prob = blockIdx.y;
-  const int yA = prob * S * P.Mpad, yB = prob * S * P.NBpad;
+  const int tiles_per_prob = tiles_m * (P.NBpad / OZ_BN);
+  // this CTA's tiles: blockIdx.x, blockIdx.x + gridDim.x, ... of all problems' tiles
+  const int my_tiles = (tiles_per_prob * P.nprob - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  struct Tile {
+    int prob, m0, n0;   // n0 in real columns of C'
+  };
+  auto tile_of = [&](int j) {
+    const int t = (int)blockIdx.x + j * (int)gridDim.x;
+    const int prob = t / tiles_per_prob, r = t % tiles_per_prob;
+    return Tile{prob, (r % tiles_m) * OZ_BM, (r / tiles_m) * OZ_BN};
+  };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; ++s) {
@@ -331,6 +346,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       mbar_init(empty + s, 1);
     }
     mbar_init(accum, 1);
+    mbar_init(drained, OZ_EPI_WARPS);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -345,98 +361,113 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   const uint32_t tmem = *tmem_holder;
 
   if (warp == 0) {
-    // ---- TMA producer
+    // ---- TMA producer: the stage ring runs on across tiles, so the next tile's first stages
+    // load while the epilogue drains the current one
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
       asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
-      int issued = 0;
-      for (int kb = 0; kb < P.kstages; ++kb) {
-        const int s = kb % ST;
-        const uint32_t ph = (kb / ST) & 1;
-        if (!mbar_wait(empty + s, ph ^ 1) || *abort_flag) {
-          *abort_flag = 1;
-          break;
+      int g = 0;   // stages issued so far (all tiles)
+      for (int j = 0; j < my_tiles && !*abort_flag; ++j) {
+        const Tile tl = tile_of(j);
+        const int yA = tl.prob * S * P.Mpad + tl.m0, yB = tl.prob * S * P.NBpad + tl.n0;
+        for (int kb = 0; kb < P.kstages; ++kb, ++g) {
+          const int s = g % ST;
+          const uint32_t ph = (g / ST) & 1;
+          if (!mbar_wait(empty + s, ph ^ 1) || *abort_flag) {
+            *abort_flag = 1;
+            break;
+          }
+          unsigned char* st = smem + s * SB;
+          mbar_expect_tx(full + s, SB);
+#pragma unroll
+          for (int i = 0; i < S; ++i) tma_load_2d(st + i * A_TILE, &tmA, full + s, kb * OZ_BK, yA + i * P.Mpad);
+#pragma unroll
+          for (int i = 0; i < S; ++i)
+            tma_load_2d(st + S * A_TILE + i * B_TILE, &tmB, full + s, kb * OZ_BK, yB + i * P.NBpad);
         }
-        unsigned char* st = smem + s * SB;
-        mbar_expect_tx(full + s, SB);
-#pragma unroll
-        for (int i = 0; i < S; ++i) tma_load_2d(st + i * A_TILE, &tmA, full + s, kb * OZ_BK, yA + i * P.Mpad + m0);
-#pragma unroll
-        for (int j = 0; j < S; ++j)
-          tma_load_2d(st + S * A_TILE + j * B_TILE, &tmB, full + s, kb * OZ_BK, yB + j * P.NBpad + n0);
-        issued = kb + 1;
       }
       if (*abort_flag) {
         // let the copies already in flight land before the CTA goes away
-        for (int kb = (issued > ST ? issued - ST : 0); kb < issued; ++kb) mbar_wait(full + kb % ST, (kb / ST) & 1);
+        for (int q = (g > ST ? g - ST : 0); q < g; ++q) mbar_wait(full + q % ST, (q / ST) & 1);
       }
     }
   } else if (warp == 1) {
-    // ---- MMA issuer
+    // ---- MMA issuer: one tile's MMAs after the epilogue has drained the previous tile
     if (lane == 0) {
-      for (int kb = 0; kb < P.kstages; ++kb) {
-        const int s = kb % ST;
-        const uint32_t ph = (kb / ST) & 1;
-        if (!mbar_wait(full + s, ph) || *abort_flag) {
+      int g = 0, commits = 0;
+      bool stop = false;
+      for (int j = 0; j < my_tiles && !stop; ++j) {
+        if (j > 0 && (!mbar_wait(drained, (uint32_t)((j - 1) & 1)) || *abort_flag)) {
           *abort_flag = 1;
           break;
         }
         fence_after();
-        const uint32_t st = smem_u32(smem + s * SB);
+        for (int kb = 0; kb < P.kstages; ++kb, ++g) {
+          const int s = g % ST;
+          const uint32_t ph = (g / ST) & 1;
+          if (!mbar_wait(full + s, ph) || *abort_flag) {
+            *abort_flag = 1;
+            stop = true;
+            break;
+          }
+          fence_after();
+          const uint32_t st = smem_u32(smem + s * SB);
 #pragma unroll
-        for (int kk = 0; kk < OZ_BK / 32; ++kk) {
+          for (int kk = 0; kk < OZ_BK / 32; ++kk) {
 #pragma unroll
-          for (int i = 0; i < S; ++i) {
-            // Row i of the slice triangle: A_i times B_0 .. B_{S-1-i}.  The B slice tiles of a
-            // stage are consecutive 64-row blocks of one swizzled operand, and the level
-            // accumulators are consecutive OZ_BN-column blocks of TMEM, so A_i [B_j .. B_{j+n-1}]
-            // is one MMA with N = n * OZ_BN whose output columns start at level i + j: the
-            // products land in their levels without any per-level MMA.
-            const uint64_t ad = smem_desc_sw64(st + i * A_TILE + kk * 32);
-            const int nmma = (S - i + OZ_SLICES_PER_MMA - 1) / OZ_SLICES_PER_MMA;
+            for (int i = 0; i < S; ++i) {
+              // Row i of the slice triangle: A_i times B_0 .. B_{S-1-i}.  The B slice tiles of a
+              // stage are consecutive 64-row blocks of one swizzled operand, and the level
+              // accumulators are consecutive OZ_BN-column blocks of TMEM, so A_i [B_j .. B_{j+n-1}]
+              // is one MMA with N = n * OZ_BN whose output columns start at level i + j: the
+              // products land in their levels without any per-level MMA.
+              const uint64_t ad = smem_desc_sw64(st + i * A_TILE + kk * 32);
+              const int nmma = (S - i + OZ_SLICES_PER_MMA - 1) / OZ_SLICES_PER_MMA;
 #pragma unroll
-            for (int q = 0; q < (S + OZ_SLICES_PER_MMA - 1) / OZ_SLICES_PER_MMA; ++q) {
-              if (q >= nmma) break;
-              const int j = q * OZ_SLICES_PER_MMA;
-              const int nj = (S - i - j) < OZ_SLICES_PER_MMA ? (S - i - j) : OZ_SLICES_PER_MMA;
-              const uint64_t bd = smem_desc_sw64(st + S * A_TILE + j * B_TILE + kk * 32);
-              const uint32_t acc = (kb > 0 || kk > 0 || i > 0) ? 1u : 0u;   // i == 0 opens every level
-              const uint32_t td = tmem + (uint32_t)((i + j) * OZ_BN);
-              const uint32_t id = idesc_i8(nj * OZ_BN);
-              // A_i is shared by the nmma products of this row
-              if (nmma == 1) mma_i8<0>(td, ad, bd, id, acc);
-              else if (q == 0) mma_i8<1>(td, ad, bd, id, acc);
-              else if (q == nmma - 1) mma_i8<3>(td, ad, bd, id, acc);
-              else mma_i8<2>(td, ad, bd, id, acc);
+              for (int q = 0; q < (S + OZ_SLICES_PER_MMA - 1) / OZ_SLICES_PER_MMA; ++q) {
+                if (q >= nmma) break;
+                const int jb = q * OZ_SLICES_PER_MMA;
+                const int nj = (S - i - jb) < OZ_SLICES_PER_MMA ? (S - i - jb) : OZ_SLICES_PER_MMA;
+                const uint64_t bd = smem_desc_sw64(st + S * A_TILE + jb * B_TILE + kk * 32);
+                const uint32_t acc = (kb > 0 || kk > 0 || i > 0) ? 1u : 0u;   // i == 0 opens every level
+                const uint32_t td = tmem + (uint32_t)((i + jb) * OZ_BN);
+                const uint32_t id = idesc_i8(nj * OZ_BN);
+                // A_i is shared by the nmma products of this row
+                if (nmma == 1) mma_i8<0>(td, ad, bd, id, acc);
+                else if (q == 0) mma_i8<1>(td, ad, bd, id, acc);
+                else if (q == nmma - 1) mma_i8<3>(td, ad, bd, id, acc);
+                else mma_i8<2>(td, ad, bd, id, acc);
+              }
             }
           }
+          mma_commit(empty + s);   // the stage's smem is free once these MMAs have read it
         }
-        mma_commit(empty + s);   // the stage's smem is free once these MMAs have read it
+        mma_commit(accum);         // this tile's MMAs (also those issued before an abort)
+        ++commits;
       }
-      mma_commit(accum);         // every MMA of this CTA done (also on the abort path)
+      if (*abort_flag && commits == 0) {
+        mma_commit(accum);
+        ++commits;
+      }
+      // no MMA may still write TMEM when it is released
+      if (commits > 0) mbar_wait(accum, (uint32_t)((commits - 1) & 1));
     }
-  }
-  // ---- epilogue, all eight warps once the accumulators are complete: warp w reads TMEM lanes
-  // 32*(w%4) .. +31 (rows m0 + 32*(w%4) + lane, the lane quarter a warp may access) and the
-  // 32-column half w/4 of every level
-  __syncwarp();
-  {
-    const int quarter = warp % 4, half = warp / 4;
-    bool ok = true;
-    if (lane == 0) ok = mbar_wait(accum, 0);   // one poller per warp
-    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-    fence_after();
-    if (!ok) *abort_flag = 1;
-    const int row = 32 * quarter + lane;
-    const int m = m0 + row;
+  } else if (warp >= 4) {
+    // ---- epilogue, eight warps: warp w reads TMEM lanes 32*(w%4) .. +31 (rows m0 + 32*(w%4) +
+    // lane, the lane quarter a warp may access) and the 32-column half (w-4)/4 of every level
+    const int quarter = warp % 4, half = (warp - 4) / 4;
     const uint32_t tbase = tmem + ((uint32_t)(32 * quarter) << 16);
-    const int Ea = P.ea[(int64_t)prob * P.Mpad + m];
-    const int* eb = P.eb + (int64_t)prob * (P.NBpad / 2);
-    cd* Cp = P.C + (int64_t)prob * P.c_bat;
     const bool use_beta = (P.beta.x != 0.0) || (P.beta.y != 0.0);
-    const bool good = ok && !*abort_flag;
-    static_assert(OZ_BN == 64, "two 32-column halves, one per group of four warps");
-    {
+    for (int j = 0; j < my_tiles; ++j) {
+      const Tile tl = tile_of(j);
+      bool ok = true;
+      if (lane == 0) ok = mbar_wait(accum, (uint32_t)(j & 1)) && !*abort_flag;   // one poller per warp
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      fence_after();
+      if (!ok) {
+        *abort_flag = 1;
+        break;
+      }
       double acc[32];
 #pragma unroll
       for (int c = 0; c < 32; ++c) acc[c] = 0.0;
@@ -449,8 +480,16 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 #pragma unroll
         for (int c = 0; c < 32; ++c) acc[c] += (double)v[c] * w;
       }
-      if (good && m < P.M) {
-        const int nbase = (n0 + half * 32) / 2;   // first complex column of this half
+      // this warp's reads of the accumulators are complete: the next tile may overwrite them
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(drained);
+      const int m = tl.m0 + 32 * quarter + lane;
+      if (m < P.M) {
+        const int Ea = P.ea[(int64_t)tl.prob * P.Mpad + m];
+        const int* eb = P.eb + (int64_t)tl.prob * (P.NBpad / 2);
+        cd* Cp = P.C + (int64_t)tl.prob * P.c_bat;
+        const int nbase = (tl.n0 + half * 32) / 2;   // first complex column of this half
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
           const int n = nbase + c;
@@ -532,6 +571,18 @@ int make_map(CUtensorMap* map, const int8_t* base, int64_t kp, int64_t rows, int
     return MPSB_ERR_CUDA;
   }
   return MPSB_OK;
+}
+
+// SMs of the current device (cached per device)
+int device_sm_count() {
+  static std::mutex mu;
+  static int count[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  std::lock_guard<std::mutex> lock(mu);
+  if (count[dev] <= 0 && cudaDeviceGetAttribute(&count[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    count[dev] = 0;
+  return count[dev] > 0 ? count[dev] : 148;
 }
 
 typedef void (*OzKernel)(CUtensorMap, CUtensorMap, OzParams);
@@ -659,8 +710,10 @@ int ozgemm_launch(const Gemm& g, int slices, void* scratch, size_t scratch_bytes
   P.err = err;
   OzKernel fn = pick_gemm(S);
   MPSB_TRY(ensure_kernel_attrs((const void*)fn, smem_of(S)));
-  const int64_t tiles = (Mpad / OZ_BM) * (NBpad / OZ_BN);
+  const int64_t tiles = (Mpad / OZ_BM) * (NBpad / OZ_BN) * B;   // output tiles of all problems
   if (tiles >= (int64_t(1) << 31)) return MPSB_ERR_UNSUPPORTED;
+  P.nprob = (int)B;
+  const int grid = (int)std::min<int64_t>(tiles, device_sm_count());   // one persistent CTA per SM
   count_launch(ws);
   Workspace::TimedLaunch ev{nullptr, nullptr, 0.0};
   const bool timed = ws && ws->prof && !ws->capturing;
@@ -671,7 +724,7 @@ int ozgemm_launch(const Gemm& g, int slices, void* scratch, size_t scratch_bytes
     // S(S+1)/2 slice products of the real (M x 2K) x (2K x 2N) GEMM per problem, 2 ops per MAC
     ev.ops = 2.0 * (S * (S + 1) / 2) * (double)g.M * (2.0 * g.N) * (2.0 * g.K) * (double)B;
   }
-  fn<<<dim3((unsigned)tiles, bz), OZ_THREADS, smem_of(S), s>>>(ta, tb, P);
+  fn<<<dim3((unsigned)grid), OZ_THREADS, smem_of(S), s>>>(ta, tb, P);
   MPSB_CUDA_TRY(cudaGetLastError());
   if (timed) {
     MPSB_CUDA_TRY(cudaEventRecord(ev.stop, s));
