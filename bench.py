@@ -891,7 +891,8 @@ def run_batch(args, rank, world, local_rank, dist):
     flops_step = batch_flops(W, chis)
 
     def timed(slices, sample_clocks=False, profile=False, e2e=False):
-        tb = BT.TrajectoryBatch(p, chis, W["dt"], r1, r2, device=local_rank, slices=slices)
+        # the sliced arms take the autotuner's per-bucket choice (mpsb200/tuning_b200.json)
+        tb = BT.TrajectoryBatch(p, chis, W["dt"], r1, r2, device=local_rank, slices=slices, tuned=slices > 0)
         if e2e:   # the example loop: the step's generators uploaded from host memory every step
             host = [tb.generator_sites(i * W["dt"]) for i in range(n)]
             run = lambda i: tb.step(host[i])   # noqa: E731

@@ -74,6 +74,12 @@ int mpsb_ctx_set_pipeline(mpsb_ctx* ctx, int enable);
  * (Complex{Float64}, or Complex{Float32} in its GPU examples,
  * examples/rydberg_density_matrix_gpu.jl:124-125); this setting has no direct counterpart. */
 int mpsb_ctx_set_precision(mpsb_ctx* ctx, int slices, int min_tiles);
+/* The sliced-path threshold of batched calls (calls on batch handles, no reference
+ * counterpart): there a GEMM takes the int8 path when one copy's problem has at least
+ * `min_flops` = 8 M N K real flops (and K >= 16), a rule that does not depend on the number of
+ * copies, so a copy computes the same bits in a batch of any size.  Default 2^24.  The
+ * autotuner of mpsb200.autotune picks it per bucket shape. */
+int mpsb_ctx_set_batched_split_threshold(mpsb_ctx* ctx, double min_flops);
 /* Device-time accounting of the sliced path's tensor-core GEMM kernel (no reference
  * counterpart): while enabled, every eager launch of that kernel is bracketed by CUDA events;
  * mpsb_ctx_profile_read waits for the context, returns the summed milliseconds, the number of

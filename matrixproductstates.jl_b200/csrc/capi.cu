@@ -253,6 +253,16 @@ int mpsb_ctx_set_precision(mpsb_ctx* ctx, int slices, int min_tiles) {
   return MPSB_OK;
 }
 
+int mpsb_ctx_set_batched_split_threshold(mpsb_ctx* ctx, double min_flops) {
+  if (!ctx) return MPSB_ERR_INVALID_ARG;
+  if (!(min_flops >= 0.0) || min_flops > 9.0e18) {
+    set_last_message("batched split threshold must be a flop count in [0, 9e18]");
+    return MPSB_ERR_INVALID_ARG;
+  }
+  ctx->split_min_flops = min_flops;
+  return MPSB_OK;
+}
+
 int mpsb_ctx_set_pipeline(mpsb_ctx* ctx, int enable) {
   if (!ctx) return MPSB_ERR_INVALID_ARG;
   ctx->pipeline = enable != 0;

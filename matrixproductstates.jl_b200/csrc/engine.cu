@@ -82,7 +82,7 @@ static int call_batch(std::initializer_list<const mpsb_mps*> mps, std::initializ
 // Whether a sweep GEMM takes the sliced path: by its output tiles (a plain call), or -- in a
 // batched call, where the decision must not depend on the batch size -- by its own work alone.
 static bool split_worth(const mpsb_ctx* ctx, const Gemm& g) {
-  if (ctx->ws.per_problem) return 8.0 * g.M * g.N * g.K >= (double)(1 << 24) && g.K >= 16;
+  if (ctx->ws.per_problem) return 8.0 * g.M * g.N * g.K >= ctx->split_min_flops && g.K >= 16;
   const int64_t tiles = ((int64_t)(g.M + 127) / 128) * ((2 * (int64_t)g.N + 63) / 64);
   return tiles >= ctx->split_min_tiles && g.K >= 16;
 }
@@ -549,7 +549,7 @@ int compress_var_apply_H(mpsb_ctx* ctx, mpsb_mps* A0, mpsb_env* envop, const mps
   bool batched;
   MPSB_TRY(call_batch({A0, Ain, A}, {envop}, &B, &batched));
   BatchScope bscope(ctx, B, batched);
-  std::vector<int64_t> key = {2, ctx->split_slices, ctx->split_min_tiles, B, maxsweeps, A0->serial, envop->serial,
+  std::vector<int64_t> key = {2, ctx->split_slices, ctx->split_min_tiles, (int64_t)ctx->split_min_flops, B, maxsweeps, A0->serial, envop->serial,
                               Ain->serial, A->serial, H->serial};
   return run_cached(ctx, key, [&]() { return compress_var_apply_H_body(ctx, A0, envop, Ain, A, H, maxsweeps); });
 }
@@ -848,7 +848,8 @@ int rk4_step(mpsb_ctx* ctx, double dt, const mpsb_mpo* H1, const mpsb_mpo* H2, c
   BatchScope bscope(ctx, B, batched);
   int64_t dtbits;
   std::memcpy(&dtbits, &dt, sizeof(dt));
-  std::vector<int64_t> key = {1, ctx->pipeline ? 2 : 1, ctx->split_slices, ctx->split_min_tiles, B, dtbits,
+  std::vector<int64_t> key = {1, ctx->pipeline ? 2 : 1, ctx->split_slices, ctx->split_min_tiles,
+                               (int64_t)ctx->split_min_flops, B, dtbits,
                               H1->serial, H2->serial, H3->serial, psi0->serial, psi->serial, psi1->serial,
                               psi2->serial, psi3->serial, env1->serial, env2->serial, env3->serial, envop->serial};
   return run_cached(ctx, key, [&]() {

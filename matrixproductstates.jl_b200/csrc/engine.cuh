@@ -25,6 +25,7 @@ struct mpsb_ctx {
   // with that many slices per operand, used for GEMMs of at least split_min_tiles output tiles
   int split_slices = 0;
   int split_min_tiles = 64;
+  double split_min_flops = 16777216.0;   // batched calls: one copy's 8 M N K at least this
   bool split_on = false;       // set while a sweep entry point issues its contractions
   // batched calls: every MPS / environment handle of the call holds `batch` copies of the same
   // shape back to back, and each kernel runs all copies at once.  The registry maps the base of

@@ -162,6 +162,10 @@ end
 set_precision!(ctx::Ctx, slices::Integer, min_tiles::Integer = 64) =
     check(ccall((:mpsb_ctx_set_precision, LIB), Cint, (Ptr{Cvoid}, Cint, Cint), ctx.h, slices, min_tiles),
           :mpsb_ctx_set_precision)
+# batched calls: the sliced path from min_flops = 8 M N K of one copy's GEMM (the autotuned value)
+set_batched_split_threshold!(ctx::Ctx, min_flops::Real) =
+    check(ccall((:mpsb_ctx_set_batched_split_threshold, LIB), Cint, (Ptr{Cvoid}, Cdouble), ctx.h, min_flops),
+          :mpsb_ctx_set_batched_split_threshold)
 
 # B copies of the sites A (a batch handle: every engine call on it runs all copies per kernel)
 function DMPS(ctx::Ctx, A::Vector{<:Array{ComplexF64,3}}, B::Integer)

@@ -37,6 +37,7 @@ SIGNATURES = {
     "mpsb_ctx_set_graphs": ([_vp, _i], _i),
     "mpsb_ctx_set_pipeline": ([_vp, _i], _i),
     "mpsb_ctx_set_precision": ([_vp, _i, _i], _i),
+    "mpsb_ctx_set_batched_split_threshold": ([_vp, _d], _i),
     "mpsb_wait_selftest": ([_vp, _d], _i),
     "mpsb_ctx_set_profiling": ([_vp, _i], _i),
     "mpsb_ctx_profile_read": ([_vp, _pd, _pi64, _pd], _i),

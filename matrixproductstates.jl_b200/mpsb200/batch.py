@@ -24,6 +24,7 @@ state do not depend on which other trajectories share its bucket.
 """
 import numpy as np
 
+from . import autotune as AT
 from . import core as K
 from . import models as Mo
 
@@ -40,7 +41,7 @@ def dims_rule(na, dmax, d):
 class TrajectoryBucket:
     """All trajectories of one bond-dim cap `chi`: the example's buffers as batch handles."""
 
-    def __init__(self, p, chi, dt, r1, r2, device=0, ctx=None, slices=0):
+    def __init__(self, p, chi, dt, r1, r2, device=0, ctx=None, slices=0, tuned=False):
         self.p, self.chi, self.dt = p, int(chi), dt
         # every copy's own uniform streams and step index (copies may start at different steps
         # when a serving loop hands a slot to a new job, see assign)
@@ -51,7 +52,10 @@ class TrajectoryBucket:
         self.active = np.ones(self.B, dtype=bool)
         self.ctx = ctx or K.Context(device)
         self.own_ctx = ctx is None
-        self.ctx.set_precision(slices)
+        # tuned: the autotuner's (slices, threshold) for this shape (mpsb200.autotune)
+        self.slices = AT.apply(self.ctx, "trajectory", 2, 4, self.chi, slices) if tuned else slices
+        if not tuned:
+            self.ctx.set_precision(slices)
         na = p.na
         dims = dims_rule(na, self.chi, 2)
         self.dims = dims
@@ -180,11 +184,13 @@ class DensityBucket:
     are handed to jobs (assign) and given back (release) by a serving loop; each copy counts its
     own steps."""
 
-    def __init__(self, p, chi, dt, B, w=8, device=0, ctx=None, slices=0):
+    def __init__(self, p, chi, dt, B, w=8, device=0, ctx=None, slices=0, tuned=False):
         self.p, self.chi, self.dt, self.B, self.w = p, int(chi), dt, int(B), int(w)
         self.ctx = ctx or K.Context(device)
         self.own_ctx = ctx is None
-        self.ctx.set_precision(slices)
+        self.slices = AT.apply(self.ctx, "density", 4, self.w, self.chi, slices) if tuned else slices
+        if not tuned:
+            self.ctx.set_precision(slices)
         na, c = p.na, self.ctx
         dims = dims_rule(na, self.chi, 4)
         self.dims = dims
@@ -238,14 +244,14 @@ class TrajectoryBatch:
     r1[k], r2[k]; grouped into buckets of equal cap; `slices` > 0 puts the sweeps' larger
     contractions on the int8-sliced tensor-core path (see Context.set_precision)."""
 
-    def __init__(self, p, chis, dt, r1, r2, device=0, slices=0):
+    def __init__(self, p, chis, dt, r1, r2, device=0, slices=0, tuned=False):
         self.p, self.dt = p, dt
         self.chis = [int(c) for c in chis]
         r1, r2 = np.asarray(r1), np.asarray(r2)
         self.members = {}
         for k, c in enumerate(self.chis):
             self.members.setdefault(c, []).append(k)
-        self.buckets = {c: TrajectoryBucket(p, c, dt, r1[m], r2[m], device, slices=slices)
+        self.buckets = {c: TrajectoryBucket(p, c, dt, r1[m], r2[m], device, slices=slices, tuned=tuned)
                         for c, m in sorted(self.members.items())}
 
     def generator_sites(self, t):

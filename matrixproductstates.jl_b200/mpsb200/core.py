@@ -55,6 +55,11 @@ class Context:
         with that many slices per operand for GEMMs of at least ``min_tiles`` output tiles."""
         _lib.call("mpsb_ctx_set_precision", self.h, int(slices), int(min_tiles))
 
+    def set_batched_split_threshold(self, min_flops):
+        """Batched calls: a GEMM takes the int8-sliced path from ``min_flops`` = 8 M N K of one
+        copy's problem (default 2^24; the per-bucket choice of ``mpsb200.autotune``)."""
+        _lib.call("mpsb_ctx_set_batched_split_threshold", self.h, float(min_flops))
+
     def set_profiling(self, enable):
         """Bracket every eager launch of the sliced path's tensor-core GEMM kernel with CUDA
         events (read with ``profile_read``)."""

@@ -150,7 +150,7 @@ class _Bucket:
     """The bucket of one job shape (see the module docstring): batch handles on its own context,
     slots handed to jobs."""
 
-    def __init__(self, key, nslots, device, slices):
+    def __init__(self, key, nslots, device, slices, tuned=True):
         kind, na, chi, dt = key
         self.key, self.kind, self.bytes = key, kind, 0
         self.ctx = K.Context(device)
@@ -159,11 +159,11 @@ class _Bucket:
             if kind == "trajectory":
                 p = Mo.WaveguideChain(na, omega=0.5)
                 z = np.zeros((nslots, 1))
-                self.eng = BT.TrajectoryBucket(p, chi, dt, z, z, device, ctx=self.ctx, slices=slices)
+                self.eng = BT.TrajectoryBucket(p, chi, dt, z, z, device, ctx=self.ctx, slices=slices, tuned=tuned)
                 self.eng.active[:] = False
             else:
                 p = Mo.WaveguideChain(na, gam_eg=0.1, omega=0.5, gam_phi=0.1)
-                self.eng = BT.DensityBucket(p, chi, dt, nslots, 8, device, ctx=self.ctx, slices=slices)
+                self.eng = BT.DensityBucket(p, chi, dt, nslots, 8, device, ctx=self.ctx, slices=slices, tuned=tuned)
         except BaseException:
             self.close()
             raise
@@ -195,14 +195,15 @@ class Server:
     max_jobs: running jobs at most; hbm_bytes: device-memory budget (default 80% of what is free);
     mode: "shared" (jobs of one shape share a bucket of the batched engine) or "per_job";
     slots: copies of a shared bucket at most; slices: int8 slices of the shared buckets' larger
-    contractions (0: FP64), as Context.set_precision."""
+    contractions (0: FP64), as Context.set_precision; tuned: each shared bucket takes the
+    autotuner's choice for its shape (mpsb200.autotune)."""
 
-    def __init__(self, device=0, max_jobs=8, hbm_bytes=None, mode="shared", slots=8, slices=6):
+    def __init__(self, device=0, max_jobs=8, hbm_bytes=None, mode="shared", slots=8, slices=6, tuned=True):
         import torch
         if mode not in ("shared", "per_job"):
             raise ValueError("mode must be 'shared' or 'per_job'")
         self.device, self.max_jobs, self.mode = device, max_jobs, mode
-        self.slots, self.slices = int(slots), int(slices)
+        self.slots, self.slices, self.tuned = int(slots), int(slices), bool(tuned)
         if hbm_bytes is None:
             free, _ = torch.cuda.mem_get_info(device)
             hbm_bytes = int(0.8 * free)
@@ -280,7 +281,7 @@ class Server:
                     if used + footprint(job, n) > self.budget:
                         break
                     try:
-                        bk = _Bucket(key, n, self.device, self.slices)
+                        bk = _Bucket(key, n, self.device, self.slices, self.tuned)
                     except _lib.MpsbError as e:
                         pending.pop(0)
                         failed.append({"job_id": job.job_id, "step": -1, "error": str(e)})
