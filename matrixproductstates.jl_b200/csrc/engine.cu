@@ -264,6 +264,7 @@ int run_qr(mpsb_ctx* ctx, const QrProblem& p0) {
   }
   void* before = ctx->ws.qr.p;
   void* before_sk = ctx->ws.splitk.p;
+  void* before_side = ctx->ws.qr_side_ws ? ctx->ws.qr_side_ws->splitk.p : nullptr;
   int st = MPSB_OK;
   for (int b = 0; b < loops && st == MPSB_OK; ++b) {
     QrProblem q = p;
@@ -275,7 +276,8 @@ int run_qr(mpsb_ctx* ctx, const QrProblem& p0) {
     count_launch(&ctx->ws);
     st = qr_launch(q, &ctx->ws, ctx->stream);
   }
-  if (ctx->ws.qr.p != before || ctx->ws.splitk.p != before_sk) ctx->ws_generation++;
+  void* after_side = ctx->ws.qr_side_ws ? ctx->ws.qr_side_ws->splitk.p : nullptr;
+  if (ctx->ws.qr.p != before || ctx->ws.splitk.p != before_sk || after_side != before_side) ctx->ws_generation++;
   return st;
 }
 

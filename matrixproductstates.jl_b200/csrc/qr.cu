@@ -842,13 +842,41 @@ int form_q(const QrProblem& p, int nb, const cd* Vb, const cd* Tb, cd* Gb, cd* M
 // formed from all reflectors as in the single-kernel path.
 constexpr int BP = 16;
 
+// The look-ahead lane of the blocked QR: created by the first (eager) call of a workspace.
+int qr_side_lane(Workspace* ws) {
+  if (ws->qr_side) return MPSB_OK;
+  if (ws->capturing) {
+    set_last_message("QR look-ahead lane first needed during graph capture");
+    return MPSB_ERR_UNSUPPORTED;
+  }
+  MPSB_CUDA_TRY(cudaStreamCreateWithFlags(&ws->qr_side, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : ws->qr_ev) MPSB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  ws->qr_side_ws = new Workspace();
+  return MPSB_OK;
+}
+
+// Right-looking blocked QR with look-ahead for shapes beyond one cluster (e.g. 2048 x 512):
+// panels of BP columns, each factored by the cluster kernel.  Panel pi's block reflector
+// I - V T V^H is applied to the next panel's columns on the main stream, which then factors
+// that panel at once, while the same update of the columns after it runs on the look-ahead
+// lane -- so the latency-bound panel factorisations overlap the trailing GEMMs.  Every column
+// still gets the panels' updates in panel order (the main stream waits for the lane's update
+// of panel pi-1 before it applies panel pi to the next panel), so the result is the
+// unblocked order's.
 int qr_blocked(const QrProblem& p, Workspace* ws, cudaStream_t s) {
   const int m = p.m, n = p.n, npan = (n + BP - 1) / BP;
   const int64_t qr_ = p.q_r, qc = p.q_c;
   // scratch: V [n][m], T [npan][16][16], G and M [n][n], panel V and E [16][m], W and W2 [n][16]
+  // (the lane's trailing update), Wn and W2n [16][16] (the next panel's update)
   const size_t nV = (size_t)m * n, nT = (size_t)npan * BP * BP, nG = (size_t)n * n, nP = (size_t)m * BP,
-               nW = (size_t)n * BP;
-  MPSB_TRY(devbuf_ensure(ws, ws->qr, (nV + nT + 2 * nG + 2 * nP + 2 * nW) * sizeof(cd)));
+               nW = (size_t)n * BP, nWn = (size_t)BP * BP;
+  MPSB_TRY(devbuf_ensure(ws, ws->qr, (nV + nT + 2 * nG + 2 * nP + 2 * nW + 2 * nWn) * sizeof(cd)));
+  MPSB_TRY(qr_side_lane(ws));
+  Workspace* sw = ws->qr_side_ws;
+  sw->capturing = ws->capturing;
+  sw->per_problem = ws->per_problem;
+  cudaStream_t ls = ws->qr_side;
+  cudaEvent_t ev_v = ws->qr_ev[0], ev_t = ws->qr_ev[1];
   cd* Vb = static_cast<cd*>(ws->qr.p);
   cd* Tb = Vb + nV;
   cd* Gb = Tb + nT;
@@ -857,13 +885,17 @@ int qr_blocked(const QrProblem& p, Workspace* ws, cudaStream_t s) {
   cd* Ep = Vp + nP;
   cd* Wb = Ep + nP;
   cd* W2 = Wb + nW;
+  cd* Wn = W2 + nW;
+  cd* W2n = Wn + nWn;
   cd* A = p.Q;
   if (p.X != p.Q || p.x_r != qr_ || p.x_c != qc)
     MPSB_TRY(mat_launch(MAT_COPY, m, n, p.X, p.x_r, p.x_c, A, qr_, qc, ws, s));
   MPSB_CUDA_TRY(cudaMemsetAsync(Vb, 0, nV * sizeof(cd), s));
   const cd one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0), mone = cmk(-1.0, 0.0);
-  for (int pi = 0; pi < npan; ++pi) {
-    const int p0 = pi * BP, pw = std::min(BP, n - p0), mp = m - p0, nt = n - p0 - pw;
+
+  // factor panel pi (its columns have every earlier panel's update) and keep its V in Vb
+  auto factor = [&](int pi) -> int {
+    const int p0 = pi * BP, pw = std::min(BP, n - p0), mp = m - p0;
     Choice ch;
     if (!choose(mp, pw, ch) || ch.nb != BP) {
       set_last_message("QR panel of %d x %d does not fit the cluster kernel", mp, pw);
@@ -880,36 +912,71 @@ int qr_blocked(const QrProblem& p, Workspace* ws, cudaStream_t s) {
     MPSB_TRY(launch_factor(pp, ch, Vp, Tb + (int64_t)pi * BP * BP, s));
     MPSB_CUDA_TRY(cudaMemcpy2DAsync(Vb + p0 + (int64_t)p0 * m, (size_t)m * sizeof(cd), Vp, (size_t)mp * sizeof(cd),
                                     (size_t)mp * sizeof(cd), pw, cudaMemcpyDeviceToDevice, s));
-    if (nt <= 0) continue;
-    cd* At = A + p0 * qr_ + (int64_t)(p0 + pw) * qc;
-    {  // W = V^H A_trail
+    return MPSB_OK;
+  };
+  // columns c0 .. c0 + nc - 1 of A <- (I - V T V^H)^H applied by panel pi, on stream st
+  auto update = [&](int pi, int c0, int nc, cd* W, int ldw, cd* Wt, Workspace* w, cudaStream_t st) -> int {
+    const int p0 = pi * BP, pw = std::min(BP, n - p0), mp = m - p0;
+    const cd* V = Vb + p0 + (int64_t)p0 * m;   // rows p0.., leading dimension m
+    cd* At = A + p0 * qr_ + (int64_t)c0 * qc;
+    {  // W = V^H A_t
       Gemm g;
-      g.M = pw; g.N = nt; g.K = mp;
-      g.A = Vp; g.a_m = mp; g.a_k = 1; g.conjA = true;
+      g.M = pw; g.N = nc; g.K = mp;
+      g.A = V; g.a_m = m; g.a_k = 1; g.conjA = true;
       g.B = At; g.b_k = qr_; g.b_n = qc;
-      g.C = Wb; g.c_m = 1; g.c_n = BP;
+      g.C = W; g.c_m = 1; g.c_n = ldw;
       g.alpha = one; g.beta = zero;
-      MPSB_TRY(gemm_launch(g, ws, s));
+      MPSB_TRY(gemm_launch(g, w, st));
     }
-    {  // W2 = T^H W
+    {  // Wt = T^H W
       Gemm g;
-      g.M = pw; g.N = nt; g.K = pw;
+      g.M = pw; g.N = nc; g.K = pw;
       g.A = Tb + (int64_t)pi * BP * BP; g.a_m = BP; g.a_k = 1; g.conjA = true;
-      g.B = Wb; g.b_k = 1; g.b_n = BP;
-      g.C = W2; g.c_m = 1; g.c_n = BP;
+      g.B = W; g.b_k = 1; g.b_n = ldw;
+      g.C = Wt; g.c_m = 1; g.c_n = ldw;
       g.alpha = one; g.beta = zero;
-      MPSB_TRY(gemm_launch(g, ws, s));
+      MPSB_TRY(gemm_launch(g, w, st));
     }
-    {  // A_trail -= V W2
+    {  // A_t -= V Wt
       Gemm g;
-      g.M = mp; g.N = nt; g.K = pw;
-      g.A = Vp; g.a_m = 1; g.a_k = mp;
-      g.B = W2; g.b_k = 1; g.b_n = BP;
+      g.M = mp; g.N = nc; g.K = pw;
+      g.A = V; g.a_m = 1; g.a_k = m;
+      g.B = Wt; g.b_k = 1; g.b_n = ldw;
       g.C = At; g.c_m = qr_; g.c_n = qc;
       g.alpha = mone; g.beta = one;
-      MPSB_TRY(gemm_launch(g, ws, s));
+      MPSB_TRY(gemm_launch(g, w, st));
+    }
+    return MPSB_OK;
+  };
+
+  MPSB_TRY(factor(0));
+  bool lane_pending = false;   // the lane holds an update the main stream has not waited for
+  for (int pi = 0; pi + 1 < npan; ++pi) {
+    const int c1 = (pi + 1) * BP, nnext = std::min(BP, n - c1);
+    const int c2 = c1 + nnext, nrest = n - c2;
+    // the next panel's columns have panel pi-1's update only once the lane's update is done
+    if (lane_pending) {
+      MPSB_CUDA_TRY(cudaStreamWaitEvent(s, ev_t, 0));
+      lane_pending = false;
+    }
+    int st = MPSB_OK;
+    if (nrest > 0) {   // V_pi and T_pi are final on the main stream: fork the trailing update
+      MPSB_CUDA_TRY(cudaEventRecord(ev_v, s));
+      MPSB_CUDA_TRY(cudaStreamWaitEvent(ls, ev_v, 0));
+      st = update(pi, c2, nrest, Wb, BP, W2, sw, ls);
+      MPSB_CUDA_TRY(cudaEventRecord(ev_t, ls));   // recorded on failure too, so the join below holds
+      lane_pending = true;
+    }
+    if (st == MPSB_OK) st = update(pi, c1, nnext, Wn, BP, W2n, ws, s);
+    if (st == MPSB_OK) st = factor(pi + 1);
+    if (st != MPSB_OK) {   // never leave the lane forked
+      cudaStreamWaitEvent(s, ev_t, 0);
+      return st;
     }
   }
+  if (lane_pending) MPSB_CUDA_TRY(cudaStreamWaitEvent(s, ev_t, 0));   // join the lane
+  ws->launches += sw->launches;
+  sw->launches = 0;
   if (p.R) MPSB_TRY(mat_launch(MAT_UPPER, n, n, A, qr_, qc, p.R, p.r_r, p.r_c, ws, s));
   MPSB_TRY(mat_launch(MAT_IDENT, m, n, nullptr, 0, 0, A, qr_, qc, ws, s));
   QrProblem q = p;

@@ -32,6 +32,11 @@ struct Workspace {
     double ops;   // int8 operations of the launch
   };
   std::vector<TimedLaunch>* prof = nullptr;
+  // look-ahead lane of the blocked QR (created by its first eager call): a stream, the two events
+  // of its fork / join, and the lane's own workspace (its GEMMs' split-K partials)
+  cudaStream_t qr_side = nullptr;
+  cudaEvent_t qr_ev[2] = {nullptr, nullptr};
+  Workspace* qr_side_ws = nullptr;
 };
 
 inline void count_launch(Workspace* ws) {
@@ -57,8 +62,23 @@ inline int devbuf_ensure(Workspace* ws, DevBuf& b, size_t bytes) {
   return MPSB_OK;
 }
 
-// every device buffer of a workspace (context teardown)
+// every device buffer of a workspace, and its QR look-ahead lane (context teardown)
 inline void ws_free(Workspace& w) {
+  if (w.qr_side) {
+    cudaStreamSynchronize(w.qr_side);
+    cudaStreamDestroy(w.qr_side);
+    w.qr_side = nullptr;
+  }
+  for (cudaEvent_t& e : w.qr_ev)
+    if (e) {
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
+  if (w.qr_side_ws) {
+    ws_free(*w.qr_side_ws);
+    delete w.qr_side_ws;
+    w.qr_side_ws = nullptr;
+  }
   DevBuf* all[] = {&w.splitk, &w.qr, &w.svd, &w.oz};
   for (DevBuf* b : all) {
     if (b->p) cudaFree(b->p);
