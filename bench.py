@@ -51,6 +51,10 @@ UNIT = "site-updates/s"
 # dram__bytes_read.sum + dram__bytes_write.sum of one cluster-QR launch at the chi=128 interior
 # shape (512 x 128; the input read once, the outputs stay in L2), from one ncu capture
 QR_TRAFFIC_BYTES = 1114624
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the sliced GEMM's tensor-core
+# kernel at M=512, N=2048, K=4096 (6 slices; the chi=512 effective-operator shape), from one ncu
+# capture (251.1 MB read + 15.4 MB written); its algorithmic bytes (slices in, C out) are 243 MB
+OZ_TRAFFIC_BYTES = 266535168
 
 
 def dims_rule(na, dmax, d):
@@ -807,7 +811,7 @@ def run_ours(args, rank, world, local_rank, dist):
         ach = sg["int8_ops"] / sg["kernel_us"] / 1e6
         roofline = {"bound": "tensor", "pipe": "int8 (tcgen05 kind::i8)", "kernel": "ozgemm_kernel<%d>" % W["slices"],
                     "achieved": ach, "peak": peak, "unit": "TOP/s", "frac": ach / peak, "peak_source": src,
-                    "traffic": None,
+                    "traffic": OZ_TRAFFIC_BYTES if (sg["M"], sg["N"], sg["K"], W["slices"]) == (512, 2048, 4096, 6) else None,
                     "per_launch": "prod_LR 3-index shape M=%d N=%d K=%d: %d slice products x 2*M*2N*2K = %.3e int8 "
                                   "ops in %.1f us (CUDA events around the kernel); whole sliced GEMM incl. slicing "
                                   "%.1f us = %.1f complex TFLOP/s" % (
@@ -973,6 +977,8 @@ def run_batch(args, rank, world, local_rank, dist):
     roofline = {"bound": "tensor", "pipe": "int8 (tcgen05 kind::i8)", "kernel": "ozgemm_kernel<%d>" % W["slices"],
                 "achieved": ach, "peak": peak, "unit": "TOP/s", "frac": ach / peak if ach else None,
                 "peak_source": src, "traffic": None,
+                "traffic_note": "launches of many shapes, no single per-launch figure; at the chi=512 effective-operator "
+                                "shape one launch moves %d DRAM bytes (ncu) against 243 MB algorithmic" % OZ_TRAFFIC_BYTES,
                 "per_launch": "all %d launches of one step of the workload (every bucket, CUDA events around each "
                               "launch): %.3e int8 ops in %.2f ms" % (cnt, ops, ms)}
     line = {
