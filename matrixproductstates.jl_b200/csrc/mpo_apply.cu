@@ -6,19 +6,21 @@
 // (src/mps_base.jl:34-37), with the reference's permutedims copies folded into the
 // strides, and the site contraction of apply_site_MPOtoMPS (src/MatrixProductStates.jl:126-133).
 // K = w*d and M = w*d are small (<= 64), so the whole Op tile sits in shared memory and
-// each CTA streams a 64-wide slab of x for one y: the kernel is bandwidth-bound and reads
-// In / writes Out exactly once, coalesced along x.
+// each CTA streams a slab of x for one y: the kernel is bandwidth-bound and reads In / writes
+// Out exactly once, coalesced along x.  A thread computes 8 outputs m of one x; the slab is 64,
+// 128 or 256 wide so that every thread has outputs also when M is 8 or 16.
 #include "common.cuh"
 
 namespace mpsb {
 namespace {
 
-constexpr int TX = 64, NT = 256;
+constexpr int NT = 256;
 
 struct MpoParams {
   MpoApply a;
   int64_t op_k1, op_k2, op_m1, op_m2;
   bool k1_fast;  // In is contiguous along k1 (else along x)
+  int tx;        // x per CTA: NT / (m-groups of 8 outputs)
 };
 
 __global__ void __launch_bounds__(NT) mpo_apply_kernel(MpoParams P) {
@@ -28,6 +30,7 @@ __global__ void __launch_bounds__(NT) mpo_apply_kernel(MpoParams P) {
   cd* opS = reinterpret_cast<cd*>(smem_raw);      // [k][m]  (m fastest)
   cd* inS = opS + K * M;                           // [k][x]  (x fastest)
   const int tid = threadIdx.x;
+  const int TX = P.tx, G = NT / TX;
   const int x0 = blockIdx.x * TX;
   const int y = blockIdx.y;
   const int64_t bz = blockIdx.z;
@@ -48,11 +51,11 @@ __global__ void __launch_bounds__(NT) mpo_apply_kernel(MpoParams P) {
   }
   __syncthreads();
 
-  const int x = tid % TX, mg = tid / TX;   // 4 m-groups
+  const int x = tid % TX, mg = tid / TX;   // G m-groups
   const int gx = x0 + x;
   const bool use_beta = (a.beta.x != 0.0) || (a.beta.y != 0.0);
   cd* out = a.out + bz * a.out_b + (int64_t)y * a.out_y;
-  for (int mb = mg * 8; mb < M; mb += 32) {
+  for (int mb = mg * 8; mb < M; mb += 8 * G) {
     cd acc[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) acc[q] = cmk(0.0, 0.0);
@@ -84,6 +87,8 @@ int mpo_apply_launch_strided(const MpoApply& a, int64_t op_k1, int64_t op_k2, in
   if (a.X <= 0 || a.Y <= 0) return MPSB_OK;
   const int K = a.K1 * a.K2, M = a.M1 * a.M2;
   if (K <= 0 || M <= 0) return MPSB_ERR_DIMENSION;
+  int TX = M <= 8 ? 256 : (M <= 16 ? 128 : 64);
+  while (TX > 64 && (size_t)(K * M + K * TX) * sizeof(cd) > 200 * 1024) TX /= 2;
   size_t smem = (size_t)(K * M + K * TX) * sizeof(cd);
   if (smem > 200 * 1024) return MPSB_ERR_UNSUPPORTED;
   if (a.Y > 65535 || a.batch < 1 || a.batch > 65535) return MPSB_ERR_UNSUPPORTED;
@@ -92,6 +97,7 @@ int mpo_apply_launch_strided(const MpoApply& a, int64_t op_k1, int64_t op_k2, in
   P.a = a;
   P.op_k1 = op_k1; P.op_k2 = op_k2; P.op_m1 = op_m1; P.op_m2 = op_m2;
   P.k1_fast = (a.in_k1 == 1) && (a.in_x != 1);
+  P.tx = TX;
   dim3 grid((a.X + TX - 1) / TX, a.Y, a.batch);
   mpo_apply_kernel<<<grid, NT, smem, s>>>(P);
   MPSB_CUDA_TRY(cudaGetLastError());
