@@ -244,6 +244,34 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
   return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
+// The S digit slices of 4 consecutive complex k of row r, at byte kbyte of each slice row (8
+// bytes): A mode writes row r as [re, im] pairs; B mode writes the row pair 2r (n,re) = [re, -im]
+// and 2r+1 (n,im) = [im, re].
+template <int S, bool BMODE>
+__device__ __forceinline__ void store_digits(int8_t* __restrict__ out, int64_t rows_out, int Kp, int r, int64_t kbyte,
+                                             const cd (&x)[4], RowScale rs) {
+  int dre[4][S], dim[4][S];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    digits<S>(x[j].x, rs, dre[j]);
+    digits<S>(x[j].y, rs, dim[j]);
+  }
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    if (!BMODE) {
+      int8_t* p = out + ((int64_t)t * rows_out + r) * Kp + kbyte;
+      *reinterpret_cast<uint2*>(p) = make_uint2(pack4(dre[0][t], dim[0][t], dre[1][t], dim[1][t]),
+                                                pack4(dre[2][t], dim[2][t], dre[3][t], dim[3][t]));
+    } else {
+      int8_t* p = out + ((int64_t)t * rows_out + 2 * (int64_t)r) * Kp + kbyte;
+      *reinterpret_cast<uint2*>(p) = make_uint2(pack4(dre[0][t], -dim[0][t], dre[1][t], -dim[1][t]),
+                                                pack4(dre[2][t], -dim[2][t], dre[3][t], -dim[3][t]));
+      *reinterpret_cast<uint2*>(p + Kp) = make_uint2(pack4(dim[0][t], dre[0][t], dim[1][t], dre[1][t]),
+                                                     pack4(dim[2][t], dre[2][t], dim[3][t], dre[3][t]));
+    }
+  }
+}
+
 // Digits of a 32-row x 32-complex tile: out[t][row][k'] (K' = 2K padded to Kp, rows padded to
 // the tile grid with zeros, so every byte the GEMM reads is written).
 template <int S, bool BMODE>
@@ -273,27 +301,64 @@ __global__ void oz_split_kernel(SliceView v, const int* __restrict__ rexp0, int6
   const int rr = tid / 8, kq = (tid % 8) * 4;
   const int r = r0 + rr;
   const RowScale rs = row_scale((r < v.R) ? rexp[r] : 0);
-  int dre[4][S], dim[4][S];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const cd x = tile[rr][kq + j];
-    digits<S>(x.x, rs, dre[j]);
-    digits<S>(x.y, rs, dim[j]);
-  }
-  const int64_t kbyte = 2 * (int64_t)(k0 + kq);   // first k' of this thread (8 bytes, < Kp)
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    if (!BMODE) {   // row r: [re_k, im_k] pairs
-      int8_t* p = out + ((int64_t)t * rows_out + r) * Kp + kbyte;
-      *reinterpret_cast<uint2*>(p) = make_uint2(pack4(dre[0][t], dim[0][t], dre[1][t], dim[1][t]),
-                                                pack4(dre[2][t], dim[2][t], dre[3][t], dim[3][t]));
-    } else {        // rows 2r (n,re) = [re, -im] and 2r+1 (n,im) = [im, re]
-      int8_t* p = out + ((int64_t)t * rows_out + 2 * (int64_t)r) * Kp + kbyte;
-      *reinterpret_cast<uint2*>(p) = make_uint2(pack4(dre[0][t], -dim[0][t], dre[1][t], -dim[1][t]),
-                                                pack4(dre[2][t], -dim[2][t], dre[3][t], -dim[3][t]));
-      *reinterpret_cast<uint2*>(p + Kp) = make_uint2(pack4(dim[0][t], dre[0][t], dim[1][t], dre[1][t]),
-                                                     pack4(dim[2][t], dre[2][t], dim[3][t], dre[3][t]));
+  const cd xs[4] = {tile[rr][kq], tile[rr][kq + 1], tile[rr][kq + 2], tile[rr][kq + 3]};
+  store_digits<S, BMODE>(out, rows_out, Kp, r, 2 * (int64_t)(k0 + kq), xs, rs);
+}
+
+// Exponent scan and slicing fused, for operands whose rows fit in shared memory: a CTA holds
+// `rpc` whole rows (all Kc complex columns of the slice grid, zeros beyond K), takes each row's
+// largest exponent and writes its digits -- one read of the operand instead of two and no
+// atomics.  rpc divides 32, so the grid covers the padded rows exactly (rows >= R get exponent
+// 0 and zero digits); exponents and digits are those of the two-pass kernels.
+constexpr int OZ_FUSED_SMEM = 96 * 1024;
+template <int S, bool BMODE>
+__global__ void __launch_bounds__(256)
+    oz_slice_rows_kernel(SliceView v, int* __restrict__ rexp0, int64_t rexp_bat, int8_t* __restrict__ out0,
+                         int64_t rows_out, int Kp, int rpc) {
+  extern __shared__ __align__(16) unsigned char rows_smem[];
+  cd* tile = reinterpret_cast<cd*>(rows_smem);   // [rpc][Kc + 1]
+  __shared__ int rowE[32];
+  const int Kc = Kp / 2, ld = Kc + 1;
+  const int r0 = blockIdx.x * rpc;
+  v.X += (int64_t)blockIdx.z * v.x_bat;
+  int* rexp = rexp0 + (int64_t)blockIdx.z * rexp_bat;
+  int8_t* out = out0 + (int64_t)blockIdx.z * S * rows_out * Kp;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const bool rc = (v.x_r == 1);   // rows contiguous: consecutive threads take consecutive rows
+  const int n = rpc * Kc;
+  for (int e = tid; e < n; e += 256) {
+    int rr, k;
+    if (rc) { rr = e % rpc; k = e / rpc; }
+    else    { k = e % Kc; rr = e / Kc; }
+    const int r = r0 + rr;
+    cd x = cmk(0.0, 0.0);
+    if (r < v.R && k < v.K) {
+      x = v.X[(int64_t)r * v.x_r + (int64_t)k * v.x_k];
+      if (v.conj) x.y = -x.y;
     }
+    tile[rr * ld + k] = x;
+  }
+  __syncthreads();
+  for (int rr = warp; rr < rpc; rr += 8) {
+    int e = 0;
+    for (int k = lane; k < Kc; k += 32) {
+      const cd x = tile[rr * ld + k];
+      e = max(e, (int)((__double_as_longlong(fmax(fabs(x.x), fabs(x.y))) >> 52) & 0x7FF));
+    }
+    for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+    if (lane == 0) {
+      rowE[rr] = e;
+      if (r0 + rr < v.R) rexp[r0 + rr] = e;
+    }
+  }
+  __syncthreads();
+  const int q4 = Kc / 4;   // items of 4 complex k per row
+  for (int it = tid; it < rpc * q4; it += 256) {
+    const int rr = it / q4, kq = (it % q4) * 4;
+    const int r = r0 + rr;
+    const cd* tp = tile + rr * ld + kq;
+    const cd xs[4] = {tp[0], tp[1], tp[2], tp[3]};
+    store_digits<S, BMODE>(out, rows_out, Kp, r, 2 * (int64_t)kq, xs, row_scale(r < v.R ? rowE[rr] : 0));
   }
 }
 
@@ -587,11 +652,13 @@ int device_sm_count() {
 
 typedef void (*OzKernel)(CUtensorMap, CUtensorMap, OzParams);
 typedef void (*SplitKernel)(SliceView, const int*, int64_t, int8_t*, int64_t, int);
+typedef void (*FusedKernel)(SliceView, int*, int64_t, int8_t*, int64_t, int, int);
 
 template <int S>
 struct OzTable {
   static OzKernel gemm() { return ozgemm_kernel<S>; }
   static SplitKernel split(bool b) { return b ? oz_split_kernel<S, true> : oz_split_kernel<S, false>; }
+  static FusedKernel fused(bool b) { return b ? oz_slice_rows_kernel<S, true> : oz_slice_rows_kernel<S, false>; }
   static int smem() { return smem_bytes(S); }
 };
 
@@ -612,6 +679,16 @@ SplitKernel pick_split(int S, bool b) {
     case 5: return OzTable<5>::split(b);
     case 6: return OzTable<6>::split(b);
     case 7: return OzTable<7>::split(b);
+  }
+  return nullptr;
+}
+FusedKernel pick_fused(int S, bool b) {
+  switch (S) {
+    case 3: return OzTable<3>::fused(b);
+    case 4: return OzTable<4>::fused(b);
+    case 5: return OzTable<5>::fused(b);
+    case 6: return OzTable<6>::fused(b);
+    case 7: return OzTable<7>::fused(b);
   }
   return nullptr;
 }
@@ -667,38 +744,58 @@ int ozgemm_launch(const Gemm& g, int slices, void* scratch, size_t scratch_bytes
   int8_t* sb = sa + (size_t)B * S * Mpad * Kp;
   int* ea = reinterpret_cast<int*>(sb + (size_t)B * S * NBpad * Kp);
   int* eb = ea + B * Mpad;
-  MPSB_CUDA_TRY(cudaMemsetAsync(ea, 0, (size_t)B * (Mpad + NBpad / 2) * sizeof(int), s));
-
   // A' rows = rows m of op(A): element (m, k) at A[m a_m + k a_k]
   SliceView va{g.A, g.M, g.K, g.a_m, g.a_k, g.conjA, g.a_b};
   // B'^T rows come from columns n of op(B): element (n, k) at B[n b_n + k b_k]
   SliceView vb{g.B, g.N, g.K, g.b_n, g.b_k, g.conjB, g.b_b};
   const int kc = (int)(Kp / 2);   // complex k extent covered by the slice grid
   const unsigned bz = (unsigned)B;
-  count_launch(ws);
-  // k tiles per exponent-scan CTA: up to 8 while the grid stays above 8 CTAs per SM (the maximum
-  // is the same whatever the partition)
+  // Rows per CTA of the fused exponent-and-slice kernel: a power of two up to 32 whose rows fit
+  // its shared memory, lowered while fewer than about two CTAs per SM would be busy, but not below
+  // 8 when the rows are the contiguous index (8 rows of 16 bytes make a full line per column);
+  // 0 when that does not fit (the exponent scan and the slicing then run as two kernels).
+  // Depends on the problem's shape and layout only.
+  auto fused_rows = [&](const SliceView& v, int64_t rows_padded) {
+    const int floor_rows = (v.x_r == 1) ? 8 : 1;
+    int rpc = 32;
+    while (rpc >= floor_rows && (size_t)rpc * (kc + 1) * sizeof(cd) > (size_t)OZ_FUSED_SMEM) rpc /= 2;
+    if (rpc < floor_rows) return 0;
+    while (rpc > floor_rows && rows_padded * B / rpc < 2 * 148) rpc /= 2;
+    return rpc;
+  };
+  const int ra = fused_rows(va, Mpad), rb = fused_rows(vb, NBpad / 2);
+  if (ra == 0 || rb == 0)
+    MPSB_CUDA_TRY(cudaMemsetAsync(ea, 0, (size_t)B * (Mpad + NBpad / 2) * sizeof(int), s));
+  // k tiles per exponent-scan CTA of the two-kernel form: up to 8 while the grid stays above 8
+  // CTAs per SM (the maximum is the same whatever the partition)
   const int ktiles = (g.K + 31) / 32;
   auto kper = [&](int rows) {
     const int64_t tiles = (int64_t)((rows + 31) / 32) * ktiles * B;
     return (int)std::max<int64_t>(1, std::min<int64_t>(8, tiles / (148 * 8)));
   };
-  const int ka = kper(g.M), kb = kper(g.N);
-  oz_rowexp_kernel<<<dim3((unsigned)((g.M + 31) / 32), (unsigned)((ktiles + ka - 1) / ka), bz), 256, 0, s>>>(
-      va, ea, Mpad, ka);
-  MPSB_CUDA_TRY(cudaGetLastError());
-  count_launch(ws);
-  oz_rowexp_kernel<<<dim3((unsigned)((g.N + 31) / 32), (unsigned)((ktiles + kb - 1) / kb), bz), 256, 0, s>>>(
-      vb, eb, NBpad / 2, kb);
-  MPSB_CUDA_TRY(cudaGetLastError());
-  count_launch(ws);
-  pick_split(S, false)<<<dim3((unsigned)(Mpad / 32), (unsigned)(kc / 32), bz), 256, 0, s>>>(va, ea, Mpad, sa, Mpad,
-                                                                                          (int)Kp);
-  MPSB_CUDA_TRY(cudaGetLastError());
-  count_launch(ws);
-  pick_split(S, true)<<<dim3((unsigned)(NBpad / 64), (unsigned)(kc / 32), bz), 256, 0, s>>>(vb, eb, NBpad / 2, sb,
-                                                                                          NBpad, (int)Kp);
-  MPSB_CUDA_TRY(cudaGetLastError());
+  auto slice = [&](const SliceView& v, int* e, int64_t rows_padded, int8_t* dst, int64_t rows_out, bool bmode,
+                   int rpc) -> int {
+    count_launch(ws);
+    if (rpc > 0) {
+      FusedKernel fk = pick_fused(S, bmode);
+      const int smem = (int)((size_t)rpc * (kc + 1) * sizeof(cd));
+      MPSB_TRY(ensure_kernel_attrs((const void*)fk, OZ_FUSED_SMEM));
+      fk<<<dim3((unsigned)(rows_padded / rpc), 1, bz), 256, smem, s>>>(v, e, rows_padded, dst, rows_out, (int)Kp, rpc);
+      MPSB_CUDA_TRY(cudaGetLastError());
+      return MPSB_OK;
+    }
+    const int kp = kper(v.R);
+    oz_rowexp_kernel<<<dim3((unsigned)((v.R + 31) / 32), (unsigned)((ktiles + kp - 1) / kp), bz), 256, 0, s>>>(
+        v, e, rows_padded, kp);
+    MPSB_CUDA_TRY(cudaGetLastError());
+    count_launch(ws);
+    pick_split(S, bmode)<<<dim3((unsigned)(rows_padded / 32), (unsigned)(kc / 32), bz), 256, 0, s>>>(
+        v, e, rows_padded, dst, rows_out, (int)Kp);
+    MPSB_CUDA_TRY(cudaGetLastError());
+    return MPSB_OK;
+  };
+  MPSB_TRY(slice(va, ea, Mpad, sa, Mpad, false, ra));
+  MPSB_TRY(slice(vb, eb, NBpad / 2, sb, NBpad, true, rb));
 
   CUtensorMap ta, tb;
   MPSB_TRY(make_map(&ta, sa, Kp, B * S * Mpad, OZ_BM));
