@@ -404,7 +404,7 @@ def workload_buffers(W, ctx, slices, start=None, perturb=0.0):
 
 
 def accuracy_arms(W, steps, local_rank):
-    """The split path against FP64 where it can be judged: (1) the FP64 path from the random
+    """The split path against FP64 where the comparison is meaningful: (1) the FP64 path from the random
     start perturbed by 1e-15 relative (the sensitivity of the truncated dynamics to rounding:
     any two FP64 implementations differ by this much), (2) split and FP64 from the physical
     all-down start at the same sizes, observables after every step."""
