@@ -67,8 +67,7 @@ enum { MB_COL0 = 0, MB_COL1, MB_RS, MB_AG, MB_COUNT };
 
 struct QrParams {
   QrProblem p;
-  cd* V;     // [batch][n][ldv] explicit unit lower trapezoidal reflectors (output)
-  int64_t ldv;   // leading dimension of V (>= m; m when V is a packed output)
+  cd* V;     // [batch][n][m] explicit unit lower trapezoidal reflectors (output)
   cd* Tg;    // [batch][npanels][NB][NB] compact-WY factor of every panel (output)
   int C, npanels, ldS, ksmax;
   // shared-memory offsets (complex elements) and the byte offset of the mbarriers
@@ -563,12 +562,12 @@ __global__ void __launch_bounds__(NT, 1) qr_kernel(QrParams P) {
     }
   }
   {  // ---- V (unit lower trapezoidal, explicit), tau, and E = [I; 0] into Q (this CTA's rows)
-    cd* V = P.V + (int64_t)prob * P.ldv * n;
+    cd* V = P.V + (int64_t)prob * m * n;
     cd* Q = P.p.Q + (int64_t)prob * P.p.q_b;
     for (int e = tid; e < ROWS * n; e += NT) {
       int rr = e % ROWS, cc = e / ROWS, g = row0 + rr;
       if (g >= m) continue;
-      V[g + (int64_t)cc * P.ldv] = g < cc ? cmk(0.0, 0.0) : (g == cc ? cmk(1.0, 0.0) : S[cc * ldS + rr]);
+      V[g + (int64_t)cc * m] = g < cc ? cmk(0.0, 0.0) : (g == cc ? cmk(1.0, 0.0) : S[cc * ldS + rr]);
       Q[(int64_t)g * P.p.q_r + (int64_t)cc * P.p.q_c] = cmk(g == cc ? 1.0 : 0.0, 0.0);
     }
   }
@@ -776,12 +775,11 @@ int mat_launch(int mode, int m, int n, const cd* src, int64_t sr, int64_t sc, cd
 
 // The cluster factorisation of every problem of p: R (if requested), the explicit reflectors
 // V [batch][n][m], the panels' T [batch][npanels][nb][nb], and E = [I; 0] in p.Q.
-int launch_factor(const QrProblem& p, const Choice& ch, cd* Vb, cd* Tb, cudaStream_t s, int64_t ldv = 0) {
+int launch_factor(const QrProblem& p, const Choice& ch, cd* Vb, cd* Tb, cudaStream_t s) {
   QrParams P;
   layout(P, p.n, ch.C, 32 * ch.rpl, ch.nb);
   P.p = p;
   P.V = Vb;
-  P.ldv = ldv > 0 ? ldv : p.m;
   P.Tg = Tb;
   QrKernel fn = kernel_for(ch.rpl, ch.nb);
   if (!fn) return MPSB_ERR_UNSUPPORTED;
@@ -868,11 +866,11 @@ int qr_side_lane(Workspace* ws) {
 int qr_blocked(const QrProblem& p, Workspace* ws, cudaStream_t s) {
   const int m = p.m, n = p.n, npan = (n + BP - 1) / BP;
   const int64_t qr_ = p.q_r, qc = p.q_c;
-  // scratch: V [n][m], T [npan][16][16], G and M [n][n], the panel's E [16][m], W and W2 [n][16]
+  // scratch: V [n][m], T [npan][16][16], G and M [n][n], panel V and E [16][m], W and W2 [n][16]
   // (the lane's trailing update), Wn and W2n [16][16] (the next panel's update)
   const size_t nV = (size_t)m * n, nT = (size_t)npan * BP * BP, nG = (size_t)n * n, nP = (size_t)m * BP,
                nW = (size_t)n * BP, nWn = (size_t)BP * BP;
-  MPSB_TRY(devbuf_ensure(ws, ws->qr, (nV + nT + 2 * nG + nP + 2 * nW + 2 * nWn) * sizeof(cd)));
+  MPSB_TRY(devbuf_ensure(ws, ws->qr, (nV + nT + 2 * nG + 2 * nP + 2 * nW + 2 * nWn) * sizeof(cd)));
   MPSB_TRY(qr_side_lane(ws));
   Workspace* sw = ws->qr_side_ws;
   sw->capturing = ws->capturing;
@@ -883,7 +881,8 @@ int qr_blocked(const QrProblem& p, Workspace* ws, cudaStream_t s) {
   cd* Tb = Vb + nV;
   cd* Gb = Tb + nT;
   cd* Mb = Gb + nG;
-  cd* Ep = Mb + nG;
+  cd* Vp = Mb + nG;
+  cd* Ep = Vp + nP;
   cd* Wb = Ep + nP;
   cd* W2 = Wb + nW;
   cd* Wn = W2 + nW;
@@ -910,8 +909,9 @@ int qr_blocked(const QrProblem& p, Workspace* ws, cudaStream_t s) {
     pp.R = Ap; pp.r_r = qr_; pp.r_c = qc;   // R rows back in place (the panel's V is kept apart)
     pp.err = p.err;
     count_launch(ws);
-    // the panel's reflectors straight into their place in V (rows p0.., leading dimension m)
-    MPSB_TRY(launch_factor(pp, ch, Vb + p0 + (int64_t)p0 * m, Tb + (int64_t)pi * BP * BP, s, m));
+    MPSB_TRY(launch_factor(pp, ch, Vp, Tb + (int64_t)pi * BP * BP, s));
+    MPSB_CUDA_TRY(cudaMemcpy2DAsync(Vb + p0 + (int64_t)p0 * m, (size_t)m * sizeof(cd), Vp, (size_t)mp * sizeof(cd),
+                                    (size_t)mp * sizeof(cd), pw, cudaMemcpyDeviceToDevice, s));
     return MPSB_OK;
   };
   // columns c0 .. c0 + nc - 1 of A <- (I - V T V^H)^H applied by panel pi, on stream st
